@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the radiance path: Msamples/s (W*H*spp per
+second of render, the reference CLI's metric, src/main.zig:243-264).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+One step renders one frame of the workload.  ``value`` is measured with the
+scene resident in HBM and the frame written to device memory (CUDA events on
+the launching stream, L2 flushed by a 256 MB write before every step, max
+over ranks); ``e2e`` goes through the public C-ABI call with host buffers
+(scene upload from pinned memory, render, framebuffer read-back).  Under
+torchrun every rank renders its own frame (seed = rank): the work is
+sharded by frame with no collective on the data path (weak scaling).
+
+``--impl reference`` times the CPU restatement of the reference renderer
+(oracle/, f64, all host threads, same atomic tile scheduler) on a bounded
+random sample of the workload's pixels, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FP64_LANES_PER_SM = 64
+NOMINAL_SM_MHZ = 1965.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--workload", default="triangle_heavy", choices=["triangle_heavy", "random_spheres", "cornell"])
+    p.add_argument("--spp", type=int, default=0, help="override spp (profiling runs)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size in seconds")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
+    return p.parse_args()
+
+
+def workload(name: str, spp_override: int):
+    import zigtrace_b200 as zt
+    from zigtrace_b200 import scenes
+    build, opts = scenes.WORKLOADS[name]
+    scene = build()
+    o = zt.Options(**{k: getattr(opts, k) for k in ("width", "height", "spp", "max_depth", "seed")})
+    if spp_override:
+        o.spp = spp_override
+    return scene, o
+
+
+def describe(name, scene, o, counts):
+    desc = {
+        "triangle_heavy": "1M-triangle heightfield + 20 icospheres + 64 emissive quads, NEE+MIS",
+        "random_spheres": "random spheres (ground plane + ~320 spheres, thin lens), no emitters",
+        "cornell": "Cornell box (glass + metal sphere, ceiling area light), NEE+MIS",
+    }[name]
+    return {"workload": f"{name}: {desc}, {o.width}x{o.height}, {o.spp} spp, depth {o.max_depth}",
+            "width": o.width, "height": o.height, "spp": o.spp, "max_depth": o.max_depth,
+            "bounded_primitives": counts["bounded"], "planes": counts["planes"], "bvh_nodes": counts["nodes"],
+            "sampled_lights": counts["lights"]}
+
+
+# ------------------------------------------------------------- CPU leg ----
+def cpu_sample(scene, o, seconds: float, threads: int, rng_seed: int = 1):
+    """Oracle render of random pixels of the workload, sized to ~seconds."""
+    import numpy as np
+    import oracle as O
+    os_ = O.OracleScene.from_scene(scene)
+    npix = o.width * o.height
+    rng = np.random.default_rng(rng_seed)
+    n = 64
+    while True:
+        pix = np.sort(rng.choice(npix, size=min(n, npix), replace=False)).astype(np.uint64)
+        t0 = time.perf_counter()
+        _, st = os_.render_pixels(o.width, o.height, o.spp, o.max_depth, pix, threads=threads, seed=o.seed,
+                                  light_sampling=o.light_sampling, stats=True)
+        dt = time.perf_counter() - t0
+        if dt >= 0.8 * seconds or n >= npix:
+            return len(pix), dt, st
+        n = int(min(npix, max(n * 2, n * seconds / max(dt, 1e-3) * 1.05)))
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    scene, o = workload(args.workload, args.spp)
+    counts_scene = scene.build().counts()
+    per_step = max(args.cpu_seconds / 3.0, 2.0)
+    n_pix, _, _ = cpu_sample(scene, o, per_step, threads)  # calibration
+    import numpy as np
+    import oracle as O
+    os_ = O.OracleScene.from_scene(scene)
+    rng = np.random.default_rng(7)
+    times = []
+    for i in range(args.warmup + args.steps):
+        pix = np.sort(rng.choice(o.width * o.height, size=n_pix, replace=False)).astype(np.uint64)
+        t0 = time.perf_counter()
+        os_.render_pixels(o.width, o.height, o.spp, o.max_depth, pix, threads=threads, seed=o.seed)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    samples = n_pix * o.spp
+    value = samples / statistics.mean(times) / 1e6
+    sample_desc = f"{n_pix} random pixels x {o.spp} spp ({samples} samples) per step"
+    print(json.dumps({
+        "impl": "reference", "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * statistics.mean(times), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
+        "config": describe(args.workload, scene, o, counts_scene),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",
+                         "sample": sample_desc + "; C restatement of the reference CPU renderer (oracle/), "
+                                                 "-O3 -ffp-contract=off, atomic tile scheduler"},
+        "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# -------------------------------------------------------------- clocks ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        self.gpu = ids[local_rank] if local_rank < len(ids) else str(local_rank)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.gpu], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [[c.strip() for c in line.split(",")] for line in out.splitlines() if line.count(",") >= 8]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------- GPU leg ----
+def b200_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import zigtrace_b200 as zt
+    from zigtrace_b200 import _native as N
+    from zigtrace_b200 import workmodel
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    scene, o = workload(args.workload, args.spp)
+    o.seed = o.seed + rank  # each rank renders its own frame
+    scene.build()
+    counts = scene.counts()
+    scene.upload()
+    gcfg = zt.GpuConfig(mode=args.mode)
+    npix = o.width * o.height
+    samples = npix * o.spp
+    out = torch.empty(npix * 3, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        flush.zero_()
+        zt.render_device(scene, o, out.data_ptr(), stream.cuda_stream, gcfg)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_start.record(stream)
+    for i in range(args.steps):
+        flush.zero_()
+        k_start[i].record(stream)
+        zt.render_device(scene, o, out.data_ptr(), stream.cuda_stream, gcfg)
+        k_end[i].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    elapsed_ms = allmax(t_start.elapsed_time(t_end))
+    kernel_ms = allmax(statistics.mean(k_start[i].elapsed_time(k_end[i]) for i in range(args.steps)))
+    ms_per_step = elapsed_ms / args.steps
+    value = world * samples / (ms_per_step / 1e3) / 1e6
+    img = out.cpu().numpy()
+    assert np.isfinite(img).all(), "non-finite pixel in the framebuffer"
+
+    # ---- e2e through the public C-ABI call with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(npix * 3, dtype=torch.float64).pin_memory()
+        rec = o.record()
+        times = []
+        for i in range(args.warmup + args.steps):
+            scene.release_device()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            N.check(N.lib().zt_render_ex(scene.handle, N.ptr(rec), N.ptr(gcfg.record()),
+                                         __import__("ctypes").c_void_p(pinned.data_ptr())))
+            t1 = time.perf_counter()
+            if i >= args.warmup:
+                times.append(t1 - t0)
+        e2e_s = allmax(statistics.mean(times))
+        e2e = {"value": round(world * samples / e2e_s / 1e6, 4), "unit": "Msamples/s",
+               "h2d_bytes_per_step": scene.staging_bytes(), "d2h_bytes_per_step": npix * 3 * 8}
+        scene.upload()
+
+    # ---- CPU baseline and per-sample work from the oracle (rank 0, N=1)
+    cpu = None
+    work = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        n_pix, dt, st = cpu_sample(scene, o, args.cpu_seconds, threads)
+        cpu = {"value": round(n_pix * o.spp / dt / 1e6, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",
+               "sample": f"{n_pix} random pixels x {o.spp} spp ({n_pix * o.spp} samples), oracle C restatement "
+                         f"of the reference CPU renderer, {threads} threads, {dt:.1f} s"}
+        work = workmodel.per_sample(st, o.spp, counts["nodes"] > 0)
+
+    roofline = None
+    if work is not None:
+        sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        flop = work["flop"] * samples
+        achieved = flop / (kernel_ms / 1e3) / 1e12
+        peak = sms * FP64_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        bytes_per_launch = work["bytes"] * samples
+        roofline = {
+            "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
+                           "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
+            "algorithmic_flop_per_sample": round(work["flop"], 1),
+            "algorithmic_bytes_per_sample": round(work["bytes"], 1),
+            "kernel_ms": round(kernel_ms, 3),
+            "memory": {"achieved_gbs": round(bytes_per_launch / (kernel_ms / 1e3) / 1e9, 1), "peak_gbs": hbm,
+                       "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
+                       "note": "bytes requested from the memory system; most are served by L2"},
+            "per_sample": {k: round(v, 3) for k, v in work.items() if k not in ("flop", "bytes")},
+        }
+
+    line = {
+        "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
+        "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
+                   "mode": ["auto", "megakernel", "wavefront"][args.mode],
+                   "sharding": "one frame per rank (seed = rank), no collective"},
+        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+/*
+ * zigtrace_b200.h -- C ABI of the B200 (sm_100a) renderer for zigtrace's
+ * per-pixel radiance path.
+ *
+ * This is the drop-in boundary for avohra25/zigtrace's library API
+ * (src/root.zig:2-17): scene construction (src/scene.zig:53-96), rendering
+ * to an f64 HDR framebuffer (src/render.zig:152-180) and the 8-bit encode
+ * (src/image.zig:24-73).  Every entry point is `extern "C"`, takes plain
+ * pointers and sizes, and blocks until its result is in the caller's buffer
+ * unless it says otherwise.  All arithmetic on the path is IEEE f64 without
+ * FMA contraction, as in the reference, so images are bit-identical to the
+ * reference algorithm's for the same scene, options and seed.
+ *
+ * Errors: every call returns a zt_status; on failure zt_last_error() returns
+ * a message for the calling thread.  Status values map onto the reference's
+ * Zig error set as noted.
+ */
+#ifndef ZIGTRACE_B200_H
+#define ZIGTRACE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t zt_status;
+#define ZT_OK 0
+#define ZT_ERR_INVALID_OPTIONS (-1)     /* error.InvalidOptions, src/render.zig:153 */
+#define ZT_ERR_OUT_OF_MEMORY (-2)       /* error.OutOfMemory (host or device) */
+#define ZT_ERR_TOO_MANY_PRIMITIVES (-3) /* error.TooManyPrimitives, src/bvh.zig:44 */
+#define ZT_ERR_UNBOUNDED_SHAPE (-4)     /* error.UnboundedShape, src/bvh.zig:55 */
+#define ZT_ERR_INVALID_ARGUMENT (-5)    /* bad pointer, index or enum value */
+#define ZT_ERR_CUDA (-6)                /* a CUDA runtime call failed */
+#define ZT_ERR_TIMEOUT (-7)             /* a bounded device wait gave up */
+#define ZT_ERR_NOT_BUILT (-8)           /* render before zt_scene_build */
+
+typedef struct { double x, y, z; } zt_vec3; /* Vec3, src/vec.zig:5-8 */
+
+/* Shape, src/geometry.zig:229-248.  p[] holds
+ *   ZT_SPHERE:   center.xyz, radius (negative radius = inward normals)
+ *   ZT_TRIANGLE: v0.xyz, v1.xyz, v2.xyz
+ *   ZT_PLANE:    point.xyz, unit normal.xyz                                   */
+enum { ZT_SPHERE = 0, ZT_TRIANGLE = 1, ZT_PLANE = 2 };
+typedef struct { uint32_t kind; uint32_t material; double p[9]; } zt_shape;
+
+/* Material, src/material.zig:15-24.  color is the albedo (lambertian,
+ * metal) or the emitted radiance (emissive); param is the metal fuzz or the
+ * dielectric index of refraction. */
+enum { ZT_LAMBERTIAN = 0, ZT_METAL = 1, ZT_DIELECTRIC = 2, ZT_EMISSIVE = 3 };
+typedef struct { uint32_t kind; uint32_t reserved; zt_vec3 color; double param; } zt_material;
+
+/* CameraConfig, src/camera.zig:8-18; focus_dist is used when
+ * has_focus_dist != 0, else |look_from - look_at|. */
+typedef struct {
+  zt_vec3 look_from, look_at, up;
+  double vfov, aperture, focus_dist;
+  uint32_t has_focus_dist, reserved;
+} zt_camera_config;
+
+/* Background, src/scene.zig:15-28: ZT_BG_SOLID uses a; ZT_BG_SKY blends from
+ * horizon a to zenith b. */
+enum { ZT_BG_SOLID = 0, ZT_BG_SKY = 1 };
+typedef struct { uint32_t kind; uint32_t reserved; zt_vec3 a, b; } zt_background;
+
+/* render.Options, src/render.zig:12-23.  threads and tile_size keep their
+ * reference meaning for validation (tile_size == 0 is InvalidOptions); the
+ * device schedules its own work. */
+typedef struct {
+  uint64_t width, height, spp, max_depth, threads, seed, tile_size;
+  uint32_t light_sampling, reserved;
+} zt_options;
+
+/* Bvh.Node, src/bvh.zig:22-33 (host copy, for inspection). */
+typedef struct { zt_vec3 bmin, bmax; uint32_t first, count; } zt_bvh_node;
+/* Light, src/light.zig:30-35 (host copy, for inspection). */
+typedef struct { zt_shape shape; zt_vec3 radiance; double weight; } zt_light;
+
+/* Device-side execution choices; zero-initialised means "defaults". */
+enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2 };
+typedef struct {
+  uint32_t mode;           /* ZT_MODE_* */
+  uint32_t block_size;     /* threads per block, 0 = default */
+  uint32_t queue_capacity; /* wavefront: paths in flight, 0 = default */
+  uint32_t reserved;
+} zt_gpu_config;
+
+typedef struct zt_scene zt_scene;
+
+/* ---- Scene construction (src/scene.zig:53-96) ------------------------- */
+/* Scene.init: an empty scene with the reference defaults (camera from the
+ * origin looking down -z, vfov 60; sky background 1,1,1 -> 0.5,0.7,1.0). */
+zt_status zt_scene_create(zt_scene** out);
+void zt_scene_destroy(zt_scene* scene);
+/* Scene.addMaterial; writes the new material id. */
+zt_status zt_scene_add_material(zt_scene* scene, const zt_material* m, uint32_t* id_out);
+/* Scene.add for n shapes; planes go to the unbounded list (scene.zig:71-78).
+ * Invalidates a previous build. */
+zt_status zt_scene_add_shapes(zt_scene* scene, const zt_shape* shapes, size_t n);
+/* Scene.addQuad: corner + a*u + b*v as two triangles (scene.zig:82-88). */
+zt_status zt_scene_add_quad(zt_scene* scene, const zt_vec3* corner, const zt_vec3* u,
+                            const zt_vec3* v, uint32_t material);
+zt_status zt_scene_set_camera(zt_scene* scene, const zt_camera_config* cfg);
+zt_status zt_scene_set_background(zt_scene* scene, const zt_background* bg);
+/* Scene.build: binned-SAH BVH and the emitter table, on the host
+ * (bvh.zig:41-67, light.zig:68-94). */
+zt_status zt_scene_build(zt_scene* scene);
+
+/* ---- Inspection (Scene fields, Bvh, Lights) --------------------------- */
+zt_status zt_scene_counts(const zt_scene* scene, uint64_t* n_materials, uint64_t* n_bounded,
+                          uint64_t* n_planes, uint64_t* n_nodes, uint64_t* n_lights);
+zt_status zt_scene_bvh(const zt_scene* scene, zt_bvh_node* nodes_out, uint32_t* indices_out);
+zt_status zt_scene_lights(const zt_scene* scene, zt_light* lights_out, double* cdf_out,
+                          double* total_out);
+zt_status zt_scene_bvh_depth(const zt_scene* scene, uint64_t* depth_out);
+
+/* ---- Device residency -------------------------------------------------- */
+/* Copies the built scene to the current CUDA device (kept until the scene is
+ * changed, destroyed, or zt_scene_release_device is called). */
+zt_status zt_scene_upload(zt_scene* scene);
+zt_status zt_scene_release_device(zt_scene* scene);
+/* Bytes one upload copies host-to-device (the flattened scene is kept in
+ * pinned host memory after the first upload, so re-uploads are one copy). */
+zt_status zt_scene_upload_bytes(zt_scene* scene, uint64_t* bytes);
+
+/* ---- Rendering (src/render.zig:152-180) -------------------------------- */
+/* render.render into a caller-owned host buffer of width*height*3 doubles,
+ * row-major, top row first.  Uploads the scene if it is not resident. */
+zt_status zt_render(zt_scene* scene, const zt_options* opts, double* out_rgb);
+/* The same with explicit device choices (cfg may be NULL). */
+zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
+                       double* out_rgb);
+/* Device-resident form: d_out_rgb is a device pointer (width*height*3
+ * doubles); the work is enqueued on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) and the call returns without synchronising.  The scene
+ * must have been uploaded to the current device. */
+zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
+                           double* d_out_rgb, void* stream);
+/* First sample of every pixel on the device: primitive id of the camera
+ * ray's closest hit (bounded-shape index, or n_bounded + plane index, -1 on a
+ * miss) and the number of extension rays the path traced.  Host buffers of
+ * width*height entries. */
+zt_status zt_render_debug(zt_scene* scene, const zt_options* opts, int32_t* first_prim_out,
+                          uint32_t* path_len_out);
+/* render.traceWith (src/render.zig:61-102) n times along one ray, drawing
+ * every path from one RNG stream in sequence, as the reference's own tests
+ * do (meanRadiance, src/render.zig:290-302).  rng_state (4 x u64, the Rng.s
+ * words) is read and updated; out has n*3 doubles.  Runs on the device. */
+zt_status zt_trace_paths(zt_scene* scene, const zt_vec3* origin, const zt_vec3* dir, uint64_t* rng_state,
+                         uint64_t n, uint64_t max_depth, uint32_t light_sampling, double* out);
+/* Rng.forStream(seed, stream_index) followed by n_draws Rng.next() on the
+ * device, for n_streams consecutive stream indices starting at stream0
+ * (src/rng.zig:22-38).  out has n_streams*n_draws entries. */
+zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, uint64_t n_draws,
+                         uint64_t* out);
+
+/* ---- Output (src/image.zig:14-73) -------------------------------------- */
+/* Image.toRgb8: exposure, tonemap (0 none, 1 reinhard, 2 aces), gamma, round
+ * to u8, on the host.  rgb_out has n_pixels*3 bytes. */
+zt_status zt_image_to_rgb8(const double* pixels, uint64_t n_pixels, uint32_t tonemap, double gamma,
+                           double exposure, uint8_t* rgb_out);
+
+const char* zt_last_error(void);
+/* Library version string. */
+const char* zt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZIGTRACE_B200_H */

@@ -1,0 +1,126 @@
+"""GPU parity with the oracle (run with -m gpu on a B200).
+
+Bar: bit-exact.  The device computes the reference's f64 arithmetic with the
+same operation order and no FMA contraction, so RNG draws, first-hit
+primitive ids, path lengths and every f64 pixel must equal the oracle's.
+Small cases compare whole images; the full-size workloads compare a random
+subset of pixels re-rendered by the oracle (pixels are independent: each
+owns its RNG stream, render.zig:135), plus size-independent properties.
+"""
+import numpy as np
+import pytest
+
+import kat_scenes as K
+import oracle as O
+import zigtrace_b200 as zt
+from zigtrace_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+DEBUG_CASES = {
+    "demo": (K.demo_scene, dict(width=48, height=32, max_depth=8)),
+    "glass": (K.glass_scene, dict(width=64, height=36, max_depth=16)),
+    "lamps": (K.lamp_scene, dict(width=64, height=36, max_depth=12)),
+    "lit_room": (K.lit_room, dict(width=48, height=32, max_depth=6)),
+    "cornell": (scenes.cornell, dict(width=128, height=128, max_depth=16)),
+    "spheres": (scenes.random_spheres, dict(width=160, height=90, max_depth=50)),
+    "coincident": (lambda: K.random_shapes(7, 300), dict(width=64, height=64, max_depth=8)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(DEBUG_CASES))
+def test_first_hit_ids_and_path_lengths_bit_exact(name):
+    build, o = DEBUG_CASES[name]
+    scene = build()
+    if name == "coincident":
+        scene.camera = zt.CameraConfig(look_from=(0, 0, 30), look_at=(0, 0, 0), vfov=50)
+    scene.build()
+    fp, pl = zt.render_debug(scene, zt.Options(o["width"], o["height"], 1, o["max_depth"]))
+    ofp, opl = O.OracleScene.from_scene(scene).render_debug(o["width"], o["height"], o["max_depth"])
+    assert (fp == ofp).all()
+    assert (pl == opl).all()
+    assert (fp >= 0).sum() > 0
+
+
+def test_rng_streams_bit_exact_many_pixels():
+    got = zt.rng_streams(12345, 0, 100_000, 4)
+    for i in (0, 1, 2, 777, 65535, 99_999):
+        assert [int(x) for x in got[i]] == [int(x) for x in O.Rng.for_stream(12345, i).next_n(4)]
+
+
+@pytest.mark.parametrize("spp,light_sampling", [(4, True), (4, False)])
+def test_cornell_small_bit_exact(spp, light_sampling):
+    scene = scenes.cornell().build()
+    img = zt.render(scene, zt.Options(64, 64, spp, 16, light_sampling=light_sampling)).pixels
+    want = O.OracleScene.from_scene(scene).render(64, 64, spp, 16, light_sampling=light_sampling)
+    assert img.tobytes() == want.tobytes()
+
+
+def test_cornell_full_size_bit_exact():
+    """The Cornell workload at its full size: 256x256, 64 spp, depth 16."""
+    scene = scenes.cornell().build()
+    o = scenes.CORNELL_OPTIONS
+    img = zt.render(scene, o).pixels
+    want = O.OracleScene.from_scene(scene).render(o.width, o.height, o.spp, o.max_depth)
+    assert img.tobytes() == want.tobytes()
+
+
+def _subset_check(scene, o: zt.Options, n_pixels: int, seed: int = 0):
+    img = zt.render(scene, o).pixels
+    rng = np.random.default_rng(seed)
+    pix = np.unique(rng.integers(0, o.width * o.height, n_pixels)).astype(np.uint64)
+    want = O.OracleScene.from_scene(scene).render_pixels(o.width, o.height, o.spp, o.max_depth, pix, seed=o.seed,
+                                                         light_sampling=o.light_sampling)
+    assert img[pix.astype(np.int64)].tobytes() == want.tobytes()
+    assert np.isfinite(img).all()
+    return img
+
+
+def test_random_spheres_full_size_subset_bit_exact():
+    """1280x720, 16 spp, depth 50; 3000 random pixels re-rendered by the oracle."""
+    scene = scenes.random_spheres().build()
+    img = _subset_check(scene, scenes.SPHERES_OPTIONS, 3000)
+    assert img.mean() > 0.1
+
+
+def test_triangle_heavy_subset_bit_exact():
+    """The 1M-triangle scene at full resolution, 4 spp; 400 oracle pixels."""
+    scene = scenes.triangle_heavy().build()
+    o = zt.Options(1920, 1080, 4, 16)
+    _subset_check(scene, o, 400)
+
+
+def test_render_is_deterministic_and_seed_dependent():
+    scene = scenes.random_spheres().build()
+    o = zt.Options(320, 180, 4, 50, seed=7)
+    a = zt.render(scene, o).pixels
+    b = zt.render(scene, o).pixels
+    assert a.tobytes() == b.tobytes()
+    c = zt.render(scene, zt.Options(320, 180, 4, 50, seed=8)).pixels
+    assert a.tobytes() != c.tobytes()
+
+
+def test_render_device_on_torch_stream_matches_host_render():
+    import torch
+    scene = scenes.cornell().build()
+    o = zt.Options(96, 64, 2, 16)
+    want = zt.render(scene, o).pixels
+    scene.upload()
+    out = torch.empty(96 * 64 * 3, dtype=torch.float64, device="cuda")
+    zt.render_device(scene, o, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().reshape(-1, 3).tobytes() == want.tobytes()
+
+
+def test_edge_options():
+    scene = K.demo_scene().build()
+    assert (zt.render(scene, zt.Options(5, 3, 2, 0)).pixels == 0).all()  # max_depth 0: loop never runs
+    one = zt.render(scene, zt.Options(1, 1, 3, 8)).pixels
+    want = O.OracleScene.from_scene(scene).render(1, 1, 3, 8)
+    assert one.tobytes() == want.tobytes()
+    odd = zt.render(scene, zt.Options(37, 23, 3, 8, seed=2**64 - 1)).pixels
+    want = O.OracleScene.from_scene(scene).render(37, 23, 3, 8, seed=2**64 - 1)
+    assert odd.tobytes() == want.tobytes()
+    with pytest.raises(zt.ZigtraceError) as ei:
+        zt.render(scene, zt.Options(0, 4, 1, 1))
+    assert ei.value.name == "InvalidOptions"

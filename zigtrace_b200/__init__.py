@@ -1,0 +1,17 @@
+"""zigtrace_b200 -- B200-native (sm_100a) renderer for zigtrace's per-pixel
+radiance path, behind a mirror of the reference library API.
+
+    import zigtrace_b200 as zt
+    scene = zt.Scene()
+    white = scene.add_material(zt.Material.lambertian((0.73, 0.73, 0.73)))
+    scene.add_quad((0, 0, 0), (555, 0, 0), (0, 0, 555), white)
+    scene.build()
+    img = zt.render(scene, zt.Options(width=256, height=256, spp=64, max_depth=16))
+    rgb = img.to_rgb8(zt.Output(tonemap="aces"))
+"""
+from .api import (  # noqa: F401
+    DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, PLANE, SPHERE, TRIANGLE,
+    Background, CameraConfig, GpuConfig, Image, Material, Options, Output, Scene, Settings, ZigtraceError, plane,
+    render, render_debug, render_device, rng_streams, sphere, triangle, write_ppm)
+
+__version__ = "0.1.0"

@@ -1,0 +1,428 @@
+/*
+ * render.cu -- device residency, the radiance kernels and the render entry
+ * points of the C ABI (include/zigtrace_b200.h).
+ *
+ * Work decomposition: render.zig:104-180 hands 16x16 tiles to host threads
+ * from an atomic counter, and each pixel draws its samples from one
+ * xoshiro256++ stream seeded by (seed, pixel index) (render.zig:135).  The
+ * samples of a pixel are therefore sequential; pixels are independent.  The
+ * megakernel runs one pixel per thread, all of its samples in order, with a
+ * persistent grid that takes pixel batches from a device work counter.
+ */
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+#include <vector>
+
+#include "scene_host.h"
+#include "zt_device.cuh"
+
+using namespace zt;
+
+/* Pinned host image of the flattened scene: every device array at a 256-byte
+ * aligned offset in one block, so an upload is a single host-to-device copy
+ * from pinned memory into a single device allocation. */
+struct zt_host_staging {
+  void* pinned = nullptr;
+  size_t bytes = 0;
+  size_t off_prims = 0, off_ids = 0, off_pairs = 0, off_planes = 0, off_mats = 0, off_lights = 0, off_cdf = 0;
+  DevScene view;  /* counts, root, total; pointers unset */
+};
+
+struct zt_device_buffers {
+  int device = -1;
+  void* block = nullptr;           /* all scene arrays */
+  unsigned int* counter = nullptr; /* work counter of the persistent grid */
+  DevScene view;
+};
+
+namespace zt {
+
+static zt_status cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? ZT_ERR_OUT_OF_MEMORY : ZT_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define ZT_CUDA(call, what)                       \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+void release_device(zt_scene* s) {
+  zt_device_buffers* d = s->device;
+  if (!d) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
+  cudaFree(d->block);
+  cudaFree(d->counter);
+  if (d->device >= 0 && d->device != cur) cudaSetDevice(cur);
+  delete d;
+  s->device = nullptr;
+}
+
+void release_staging(zt_scene* s) {
+  release_device(s);
+  if (!s->staging) return;
+  cudaFreeHost(s->staging->pinned);
+  delete s->staging;
+  s->staging = nullptr;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <typename T>
+static void stage(const std::vector<T>& v, size_t& cursor, size_t& off) {
+  off = cursor;
+  cursor = align256(cursor + v.size() * sizeof(T));
+}
+
+template <typename T>
+static void stage_copy(const std::vector<T>& v, void* base, size_t off) {
+  if (!v.empty()) memcpy((char*)base + off, v.data(), v.size() * sizeof(T));
+}
+
+/* Flattens the built scene into one pinned block (once per build). */
+static zt_status make_staging(zt_scene* s) {
+  if (s->staging) return ZT_OK;
+  FlatScene f;
+  try {
+    flatten_scene(s, &f);
+  } catch (const std::bad_alloc&) {
+    return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory while flattening the scene");
+  }
+  zt_host_staging* h = new (std::nothrow) zt_host_staging();
+  if (!h) return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory");
+  size_t cur = 0;
+  stage(f.prims, cur, h->off_prims);
+  stage(f.prim_ids, cur, h->off_ids);
+  stage(f.pairs, cur, h->off_pairs);
+  stage(f.planes, cur, h->off_planes);
+  stage(f.mats, cur, h->off_mats);
+  stage(f.lights, cur, h->off_lights);
+  stage(f.cdf, cur, h->off_cdf);
+  h->bytes = cur > 0 ? cur : 256;
+  cudaError_t e = cudaMallocHost(&h->pinned, h->bytes);
+  if (e != cudaSuccess) {
+    delete h;
+    return cuda_fail(e, "allocate pinned staging");
+  }
+  memset(h->pinned, 0, h->bytes);
+  stage_copy(f.prims, h->pinned, h->off_prims);
+  stage_copy(f.prim_ids, h->pinned, h->off_ids);
+  stage_copy(f.pairs, h->pinned, h->off_pairs);
+  stage_copy(f.planes, h->pinned, h->off_planes);
+  stage_copy(f.mats, h->pinned, h->off_mats);
+  stage_copy(f.lights, h->pinned, h->off_lights);
+  stage_copy(f.cdf, h->pinned, h->off_cdf);
+  h->view = f.view;
+  s->staging = h;
+  return ZT_OK;
+}
+
+static zt_status upload(zt_scene* s) {
+  if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
+  int dev = 0;
+  ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (s->device && s->device->device == dev) return ZT_OK;
+  release_device(s);
+  zt_status rc = make_staging(s);
+  if (rc != ZT_OK) return rc;
+  const zt_host_staging* h = s->staging;
+  zt_device_buffers* d = new (std::nothrow) zt_device_buffers();
+  if (!d) return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory");
+  d->device = dev;
+  s->device = d;
+  cudaError_t e = cudaMalloc(&d->block, h->bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d->counter, 4 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemcpy(d->block, h->pinned, h->bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    release_device(s);
+    return cuda_fail(e, "upload scene");
+  }
+  char* b = (char*)d->block;
+  d->view = h->view;
+  d->view.prims = (const DPrim*)(b + h->off_prims);
+  d->view.prim_ids = (const int32_t*)(b + h->off_ids);
+  d->view.pairs = (const DPair*)(b + h->off_pairs);
+  d->view.planes = (const DPrim*)(b + h->off_planes);
+  d->view.mats = (const DMat*)(b + h->off_mats);
+  d->view.lights = (const DLight*)(b + h->off_lights);
+  d->view.cdf = (const double*)(b + h->off_cdf);
+  return ZT_OK;
+}
+
+/* The resident view with the scene's current background (the background can
+ * change after upload without touching device memory). */
+static DevScene launch_view(const zt_scene* s) {
+  DevScene v = s->device->view;
+  const zt_background& bg = s->background;
+  v.bg.kind = bg.kind;
+  v.bg.a[0] = bg.a.x; v.bg.a[1] = bg.a.y; v.bg.a[2] = bg.a.z;
+  v.bg.b[0] = bg.b.x; v.bg.b[1] = bg.b.y; v.bg.b[2] = bg.b.z;
+  return v;
+}
+
+static bool options_valid(const zt_options* o) { /* render.zig:153 */
+  return !(o->width == 0 || o->height == 0 || o->spp == 0 || o->tile_size == 0);
+}
+
+static RenderParams make_params(const zt_scene* s, const zt_options* o) {
+  RenderParams p;
+  p.cam = camera_init(s->camera, (double)o->width / (double)o->height); /* render.zig:157, 162 */
+  p.width = o->width;
+  p.height = o->height;
+  p.spp = o->spp;
+  p.max_depth = o->max_depth;
+  p.seed = o->seed;
+  p.use_nee = (o->light_sampling && !s->lights.empty()) ? 1u : 0u; /* render.zig:62 */
+  p.pad = 0;
+  return p;
+}
+
+/* ------------------------------------------------------------ Kernels ---- */
+
+/* One pixel: renderTile's per-pixel body, render.zig:133-144. */
+template <bool kAux>
+__device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderParams& p, uint64_t pix,
+                                             double* __restrict__ out, TraceAux* aux) {
+  const uint64_t x = pix % p.width, y = pix / p.width;
+  const double w = (double)p.width, h = (double)p.height;
+  const double inv_spp = 1.0 / (double)p.spp;
+  Rng rng = rng_for_stream(p.seed, y * p.width + x);
+  dv3 sum = V(0, 0, 0);
+  for (uint64_t i = 0; i < p.spp; ++i) {
+    const double s = ((double)x + rng_float(rng)) / w;
+    const double t = ((double)y + rng_float(rng)) / h;
+    dv3 ro, rd;
+    camera_ray(p.cam, s, t, rng, ro, rd);
+    const dv3 c = trace_with<kAux>(sc, ro, rd, rng, p.max_depth, p.use_nee != 0, aux);
+    if (kAux) break;
+    if (visfinite(c)) sum = sum + c;
+  }
+  if (!kAux) {
+    const dv3 px = vscale(sum, inv_spp);
+    out[3 * pix + 0] = px.x;
+    out[3 * pix + 1] = px.y;
+    out[3 * pix + 2] = px.z;
+  }
+}
+
+/* Persistent megakernel: each warp takes 32 consecutive pixels from the
+ * device work counter until the image is exhausted (the device form of
+ * Context.work's atomic tile counter, render.zig:113-119). */
+__global__ void __launch_bounds__(128) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
+                                                     unsigned int* __restrict__ counter) {
+  const uint64_t npix = p.width * p.height;
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base >= npix) return;
+    const uint64_t pix = (uint64_t)base + lane;
+    if (pix < npix) render_pixel<false>(sc, p, pix, out, nullptr);
+  }
+}
+
+__global__ void k_render_debug(DevScene sc, RenderParams p, int32_t* __restrict__ first_prim,
+                               uint32_t* __restrict__ path_len) {
+  const uint64_t pix = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= p.width * p.height) return;
+  TraceAux aux;
+  render_pixel<true>(sc, p, pix, nullptr, &aux);
+  first_prim[pix] = aux.first_prim;
+  path_len[pix] = aux.path_len;
+}
+
+__global__ void k_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, uint64_t n_draws,
+                              uint64_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_streams) return;
+  Rng r = rng_for_stream(seed, stream0 + i);
+  for (uint64_t k = 0; k < n_draws; ++k) out[i * n_draws + k] = rng_next(r);
+}
+
+/* meanRadiance's loop (render.zig:290-302): one thread, one RNG stream, n
+ * paths along the same ray in sequence. */
+__global__ void k_trace_paths(DevScene sc, double ox, double oy, double oz, double dx, double dy, double dz,
+                              uint64_t* __restrict__ rng_state, uint64_t n, uint64_t max_depth, uint32_t use_nee,
+                              double* __restrict__ out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  Rng rng{rng_state[0], rng_state[1], rng_state[2], rng_state[3]};
+  for (uint64_t i = 0; i < n; ++i) {
+    const dv3 c = trace_with<false>(sc, V(ox, oy, oz), V(dx, dy, dz), rng, max_depth, use_nee != 0, nullptr);
+    out[3 * i + 0] = c.x;
+    out[3 * i + 1] = c.y;
+    out[3 * i + 2] = c.z;
+  }
+  rng_state[0] = rng.s0;
+  rng_state[1] = rng.s1;
+  rng_state[2] = rng.s2;
+  rng_state[3] = rng.s3;
+}
+
+static int sm_count() {
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+    if (cached <= 0) cached = 1;
+  }
+  return cached;
+}
+
+static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* d_out,
+                               cudaStream_t stream) {
+  (void)cfg;
+  zt_device_buffers* d = s->device;
+  const RenderParams p = make_params(s, o);
+  ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
+  int per_sm = 0;
+  ZT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_mega, 128, 0), "occupancy query");
+  if (per_sm < 1) per_sm = 1;
+  const uint64_t npix = o->width * o->height;
+  uint64_t blocks = (uint64_t)sm_count() * per_sm;
+  const uint64_t need = (npix + 127) / 128;
+  if (blocks > need) blocks = need;
+  k_render_mega<<<(unsigned)blocks, 128, 0, stream>>>(launch_view(s), p, d_out, d->counter);
+  ZT_CUDA(cudaGetLastError(), "launch k_render_mega");
+  return ZT_OK;
+}
+
+static zt_status check_render_args(zt_scene* s, const zt_options* o) {
+  if (!s || !o) return fail(ZT_ERR_INVALID_ARGUMENT, "NULL scene or options");
+  if (!options_valid(o)) return fail(ZT_ERR_INVALID_OPTIONS, "InvalidOptions: width, height, spp and tile_size must be > 0");
+  if (o->width > (1ull << 31) || o->height > (1ull << 31) || o->width * o->height > (1ull << 31))
+    return fail(ZT_ERR_INVALID_OPTIONS, "InvalidOptions: more than 2^31 pixels");
+  if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
+  return ZT_OK;
+}
+
+}  // namespace zt
+
+extern "C" {
+
+zt_status zt_scene_upload(zt_scene* s) {
+  if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_upload: NULL scene");
+  return upload(s);
+}
+
+zt_status zt_scene_upload_bytes(zt_scene* s, uint64_t* bytes) {
+  if (!s || !bytes) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_upload_bytes: NULL argument");
+  if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
+  zt_status rc = make_staging(s);
+  if (rc != ZT_OK) return rc;
+  *bytes = s->staging->bytes;
+  return ZT_OK;
+}
+
+zt_status zt_scene_release_device(zt_scene* s) {
+  if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_release_device: NULL scene");
+  release_device(s);
+  return ZT_OK;
+}
+
+zt_status zt_render_device(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* d_out, void* stream) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!d_out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_device: NULL output");
+  int dev = 0;
+  ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (!s->device || s->device->device != dev)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "scene is not resident on the current device: call zt_scene_upload");
+  return launch_render(s, o, cfg, d_out, (cudaStream_t)stream);
+}
+
+zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* out) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render: NULL output");
+  rc = upload(s);
+  if (rc != ZT_OK) return rc;
+  const size_t bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  double* d_out = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer");
+  rc = launch_render(s, o, cfg, d_out, 0);
+  if (rc == ZT_OK) {
+    cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(e, "render / copy framebuffer");
+  }
+  cudaFree(d_out);
+  return rc;
+}
+
+zt_status zt_render(zt_scene* s, const zt_options* o, double* out) { return zt_render_ex(s, o, nullptr, out); }
+
+zt_status zt_render_debug(zt_scene* s, const zt_options* o, int32_t* first_prim, uint32_t* path_len) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!first_prim || !path_len) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_debug: NULL output");
+  rc = upload(s);
+  if (rc != ZT_OK) return rc;
+  const uint64_t npix = o->width * o->height;
+  int32_t* d_fp = nullptr;
+  uint32_t* d_pl = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d_fp, npix * sizeof(int32_t)), "allocate debug buffer");
+  cudaError_t e = cudaMalloc((void**)&d_pl, npix * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    cudaFree(d_fp);
+    return cuda_fail(e, "allocate debug buffer");
+  }
+  const RenderParams p = make_params(s, o);
+  k_render_debug<<<(unsigned)((npix + 127) / 128), 128>>>(launch_view(s), p, d_fp, d_pl);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(first_prim, d_fp, npix * sizeof(int32_t), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(path_len, d_pl, npix * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(d_fp);
+  cudaFree(d_pl);
+  if (e != cudaSuccess) return cuda_fail(e, "debug render");
+  return ZT_OK;
+}
+
+zt_status zt_trace_paths(zt_scene* s, const zt_vec3* origin, const zt_vec3* dir, uint64_t* rng_state, uint64_t n,
+                         uint64_t max_depth, uint32_t light_sampling, double* out) {
+  if (!s || !origin || !dir || !rng_state || (!out && n))
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_trace_paths: NULL argument");
+  if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
+  zt_status rc = upload(s);
+  if (rc != ZT_OK) return rc;
+  if (n == 0) return ZT_OK;
+  uint64_t* d_rng = nullptr;
+  double* d_out = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d_rng, 4 * sizeof(uint64_t)), "allocate rng state");
+  cudaError_t e = cudaMalloc((void**)&d_out, n * 3 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_rng, rng_state, 4 * sizeof(uint64_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const uint32_t use_nee = (light_sampling && !s->lights.empty()) ? 1u : 0u; /* render.zig:62 */
+    k_trace_paths<<<1, 32>>>(launch_view(s), origin->x, origin->y, origin->z, dir->x, dir->y, dir->z, d_rng, n,
+                             max_depth, use_nee, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, n * 3 * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(rng_state, d_rng, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+  cudaFree(d_rng);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return cuda_fail(e, "trace paths");
+  return ZT_OK;
+}
+
+zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, uint64_t n_draws, uint64_t* out) {
+  if (!out && n_streams * n_draws) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_rng_streams: NULL output");
+  if (n_streams == 0 || n_draws == 0) return ZT_OK;
+  const size_t bytes = (size_t)(n_streams * n_draws) * sizeof(uint64_t);
+  uint64_t* d = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d, bytes), "allocate rng buffer");
+  k_rng_streams<<<(unsigned)((n_streams + 127) / 128), 128>>>(seed, stream0, n_streams, n_draws, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out, d, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "rng streams");
+  return ZT_OK;
+}
+
+}  /* extern "C" */

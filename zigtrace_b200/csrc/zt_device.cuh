@@ -1,0 +1,542 @@
+/*
+ * zt_device.cuh -- device functions of the radiance path (f64, sm_100a).
+ *
+ * Each function restates the reference routine named beside it with the same
+ * IEEE-754 double operations in the same order.  The translation unit is
+ * compiled with -fmad=false so no multiply-add is contracted, as in the
+ * reference's strict-float Zig build; division and sqrt of doubles are the
+ * correctly rounded CUDA defaults.  The result is a bit-exact device
+ * restatement: same hits, same RNG draws, same radiance.
+ */
+#ifndef ZT_DEVICE_CUH
+#define ZT_DEVICE_CUH
+
+#include <stdint.h>
+
+#include "zt_fpmath.h"
+#include "zt_types.h"
+
+namespace zt {
+
+#define ZT_D __device__ __forceinline__
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kRayEpsilon = 1e-4;  /* render.zig:26 */
+constexpr uint64_t kRouletteDepth = 4; /* render.zig:28 */
+constexpr int kStackSize = 66;         /* bvh.zig:87: max_depth + 2 */
+
+/* ------------------------------------------------------------- Vec3 ---- */
+/* src/vec.zig:5-125 */
+struct dv3 { double x, y, z; };
+ZT_D dv3 V(double x, double y, double z) { return dv3{x, y, z}; }
+ZT_D dv3 L3(const double* p) { return dv3{p[0], p[1], p[2]}; }
+ZT_D dv3 operator+(dv3 a, dv3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+ZT_D dv3 operator-(dv3 a, dv3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+ZT_D dv3 vmul(dv3 a, dv3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+ZT_D dv3 vscale(dv3 a, double s) { return V(a.x * s, a.y * s, a.z * s); }
+ZT_D dv3 vdiv(dv3 a, double s) { return vscale(a, 1.0 / s); } /* vec.zig:37-39 */
+ZT_D dv3 vneg(dv3 a) { return V(-a.x, -a.y, -a.z); }
+ZT_D double vdot(dv3 a, dv3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+ZT_D dv3 vcross(dv3 a, dv3 b) {
+  return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+ZT_D double vlen2(dv3 a) { return vdot(a, a); }
+ZT_D double vlen(dv3 a) { return sqrt(vlen2(a)); }
+ZT_D dv3 vnorm(dv3 a) { return vdiv(a, vlen(a)); }
+ZT_D dv3 vlerp(dv3 a, dv3 b, double t) { return vscale(a, 1.0 - t) + vscale(b, t); }
+ZT_D double vmaxc(dv3 a) { return fmax(a.x, fmax(a.y, a.z)); }
+ZT_D bool vnear_zero(dv3 a) {
+  const double eps = 1e-8;
+  return fabs(a.x) < eps && fabs(a.y) < eps && fabs(a.z) < eps;
+}
+ZT_D bool visfinite(dv3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+ZT_D dv3 vreflect(dv3 v, dv3 n) { return v - vscale(n, 2.0 * vdot(v, n)); }
+ZT_D dv3 vrefract(dv3 uv, dv3 n, double eta) { /* vec.zig:119-124 */
+  const double cos_theta = fmin(vdot(vneg(uv), n), 1.0);
+  const dv3 r_perp = vscale(uv + vscale(n, cos_theta), eta);
+  const dv3 r_par = vscale(n, -sqrt(fabs(1.0 - vlen2(r_perp))));
+  return r_perp + r_par;
+}
+
+/* -------------------------------------------------------------- Rng ---- */
+/* src/rng.zig:10-88 */
+struct Rng { uint64_t s0, s1, s2, s3; };
+
+ZT_D uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+ZT_D uint64_t splitmix64(uint64_t& state) {
+  state += 0x9E3779B97F4A7C15ULL;
+  uint64_t z = state;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+ZT_D Rng rng_for_stream(uint64_t seed, uint64_t stream) { /* rng.zig:22-25 */
+  uint64_t sm = seed ^ (stream * 0x9E3779B97F4A7C15ULL);
+  uint64_t s2 = splitmix64(sm);
+  Rng r;
+  r.s0 = splitmix64(s2);
+  r.s1 = splitmix64(s2);
+  r.s2 = splitmix64(s2);
+  r.s3 = splitmix64(s2);
+  return r;
+}
+ZT_D uint64_t rng_next(Rng& r) { /* rng.zig:27-38, xoshiro256++ */
+  const uint64_t result = rotl64(r.s0 + r.s3, 23) + r.s0;
+  const uint64_t t = r.s1 << 17;
+  r.s2 ^= r.s0;
+  r.s3 ^= r.s1;
+  r.s1 ^= r.s2;
+  r.s0 ^= r.s3;
+  r.s2 ^= t;
+  r.s3 = rotl64(r.s3, 45);
+  return result;
+}
+ZT_D double rng_float(Rng& r) { return (double)(rng_next(r) >> 11) * 0x1.0p-53; }
+ZT_D double rng_range(Rng& r, double lo, double hi) { return lo + (hi - lo) * rng_float(r); }
+ZT_D dv3 rng_unit_vector(Rng& r) { /* rng.zig:58-63 */
+  const double z = rng_range(r, -1.0, 1.0);
+  const double phi = rng_range(r, 0.0, 2.0 * kPi);
+  const double rr = sqrt(fmax(0.0, 1.0 - z * z));
+  double s, c;
+  zt_sincos(phi, &s, &c);
+  return V(rr * c, rr * s, z);
+}
+ZT_D dv3 rng_in_unit_disk(Rng& r) { /* rng.zig:74-79 */
+  for (;;) {
+    const double x = rng_range(r, -1, 1);
+    const double y = rng_range(r, -1, 1);
+    if (x * x + y * y + 0.0 * 0.0 < 1.0) return V(x, y, 0);
+  }
+}
+
+/* -------------------------------------------------------------- Hit ---- */
+/* src/geometry.zig:11-30; prim is instrumentation only. */
+struct Hit {
+  double t;
+  dv3 point, normal;
+  uint32_t front_face, material;
+  int32_t prim;
+};
+
+ZT_D void hit_make(dv3 o, dv3 d, double t, dv3 outward, uint32_t mat, Hit& h) {
+  const bool front = vdot(d, outward) < 0;
+  h.t = t;
+  h.point = o + vscale(d, t); /* Ray.at, ray.zig:12-14 */
+  h.normal = front ? outward : vneg(outward);
+  h.front_face = front;
+  h.material = mat;
+}
+
+/* Sphere.intersect, geometry.zig:37-52.  Returns the root t or a value
+ * outside the range; the hit record is built only for the closest hit. */
+ZT_D bool sphere_t(dv3 center, double radius, dv3 o, dv3 d, double tmin, double tmax, double& tout) {
+  const dv3 oc = center - o;
+  const double a = vlen2(d);
+  const double h = vdot(d, oc);
+  const double c = vlen2(oc) - radius * radius;
+  const double disc = h * h - a * c;
+  if (disc < 0) return false;
+  const double sq = sqrt(disc);
+  double t = (h - sq) / a;
+  if (t <= tmin || t >= tmax) {
+    t = (h + sq) / a;
+    if (t <= tmin || t >= tmax) return false;
+  }
+  tout = t;
+  return true;
+}
+ZT_D void sphere_hit(dv3 center, double radius, uint32_t mat, dv3 o, dv3 d, double t, Hit& h) {
+  const dv3 outward = vdiv((o + vscale(d, t)) - center, radius);
+  hit_make(o, d, t, outward, mat, h);
+}
+
+/* Moller-Trumbore, geometry.zig:83-99, with e1/e2 precomputed. */
+ZT_D bool triangle_t(dv3 v0, dv3 e1, dv3 e2, dv3 o, dv3 d, double tmin, double tmax, double& tout) {
+  const dv3 p = vcross(d, e2);
+  const double det = vdot(e1, p);
+  if (fabs(det) < 1e-12) return false;
+  const double inv_det = 1.0 / det;
+  const dv3 s = o - v0;
+  const double u = vdot(s, p) * inv_det;
+  if (u < 0 || u > 1) return false;
+  const dv3 q = vcross(s, e1);
+  const double v = vdot(d, q) * inv_det;
+  if (v < 0 || u + v > 1) return false;
+  const double t = vdot(e2, q) * inv_det;
+  if (t <= tmin || t >= tmax) return false;
+  tout = t;
+  return true;
+}
+ZT_D void triangle_hit(dv3 e1, dv3 e2, uint32_t mat, dv3 o, dv3 d, double t, Hit& h) {
+  hit_make(o, d, t, vnorm(vcross(e1, e2)), mat, h);
+}
+
+/* Plane.intersect, geometry.zig:67-73. */
+ZT_D bool plane_t(dv3 point, dv3 normal, dv3 o, dv3 d, double tmin, double tmax, double& tout) {
+  const double denom = vdot(normal, d);
+  if (fabs(denom) < 1e-12) return false;
+  const double t = vdot(point - o, normal) / denom;
+  if (t <= tmin || t >= tmax) return false;
+  tout = t;
+  return true;
+}
+
+ZT_D bool prim_t(const DPrim& p, dv3 o, dv3 d, double tmin, double tmax, double& t) {
+  if (p.kind == kTriangle) return triangle_t(L3(p.a), L3(p.a + 3), L3(p.a + 6), o, d, tmin, tmax, t);
+  if (p.kind == kSphere) return sphere_t(L3(p.a), p.a[3], o, d, tmin, tmax, t);
+  return plane_t(L3(p.a), L3(p.a + 3), o, d, tmin, tmax, t);
+}
+ZT_D void prim_hit(const DPrim& p, dv3 o, dv3 d, double t, Hit& h) {
+  if (p.kind == kTriangle) triangle_hit(L3(p.a + 3), L3(p.a + 6), p.material, o, d, t, h);
+  else if (p.kind == kSphere) sphere_hit(L3(p.a), p.a[3], p.material, o, d, t, h);
+  else hit_make(o, d, t, L3(p.a + 3), p.material, h);
+}
+
+/* --------------------------------------------------------- Traversal ---- */
+/* Slab test of one box, aabb.zig:68-83.  The reference returns early once
+ * hi < lo; lo only grows and hi only shrinks afterwards, so testing once at
+ * the end is the same predicate, and `if (t0 > lo) lo = t0` equals
+ * fmax(lo, t0) including the NaN case (0 * inf leaves lo unchanged). */
+ZT_D bool slab(const double* lo3, const double* hi3, dv3 o, dv3 inv, double tmin, double tmax, double& tout) {
+  double lo = tmin, hi = tmax;
+  {
+    double t0 = (lo3[0] - o.x) * inv.x, t1 = (hi3[0] - o.x) * inv.x;
+    const bool sw = inv.x < 0;
+    lo = fmax(lo, sw ? t1 : t0);
+    hi = fmin(hi, sw ? t0 : t1);
+  }
+  {
+    double t0 = (lo3[1] - o.y) * inv.y, t1 = (hi3[1] - o.y) * inv.y;
+    const bool sw = inv.y < 0;
+    lo = fmax(lo, sw ? t1 : t0);
+    hi = fmin(hi, sw ? t0 : t1);
+  }
+  {
+    double t0 = (lo3[2] - o.z) * inv.z, t1 = (hi3[2] - o.z) * inv.z;
+    const bool sw = inv.z < 0;
+    lo = fmax(lo, sw ? t1 : t0);
+    hi = fmin(hi, sw ? t0 : t1);
+  }
+  tout = lo;
+  return !(hi < lo);
+}
+
+struct StackEntry { uint32_t first, count; double t; };
+
+/* Scene.intersect (scene.zig:108-116): Bvh.intersect (bvh.zig:80-126) with
+ * the same nearest-first order, `tl <= tr` tie-break and `entry.t > closest`
+ * pruning, then the unbounded planes up to the BVH hit.  any_hit = true stops
+ * at the first primitive hit: the traversal up to that point is identical,
+ * so whether a hit exists is the same answer the reference's closest-hit
+ * query gives to `!= null` (render.zig:51). */
+template <bool kAnyHit>
+ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, Hit& out) {
+  double closest = tmax;
+  int32_t best_k = -1;  /* >= 0: prims[best_k]; <= -2: planes[-2 - best_k] */
+  if (sc.has_root) {
+    const dv3 inv = V(1.0 / d.x, 1.0 / d.y, 1.0 / d.z);
+    StackEntry stack[kStackSize];
+    int sp = 0;
+    double t;
+    if (slab(sc.root_lo, sc.root_hi, o, inv, tmin, closest, t)) {
+      stack[0].first = sc.root_first;
+      stack[0].count = sc.root_count;
+      stack[0].t = t;
+      sp = 1;
+    }
+    while (sp > 0) {
+      --sp;
+      const StackEntry e = stack[sp];
+      if (e.t > closest) continue;
+      if (e.count > 0) {
+        for (uint32_t k = e.first; k < e.first + e.count; ++k) {
+          double th;
+          if (prim_t(sc.prims[k], o, d, tmin, closest, th)) {
+            closest = th;
+            best_k = (int32_t)k;
+            if (kAnyHit) { out.t = th; return true; }
+          }
+        }
+        continue;
+      }
+      const DPair& pr = sc.pairs[e.first];
+      double tl, tr;
+      const bool hl = slab(pr.lo[0], pr.hi[0], o, inv, tmin, closest, tl);
+      const bool hr = slab(pr.lo[1], pr.hi[1], o, inv, tmin, closest, tr);
+      if (hl && hr) {
+        const bool near_left = tl <= tr;
+        const int nf = near_left ? 1 : 0, nn = near_left ? 0 : 1;
+        stack[sp].first = pr.first[nf];
+        stack[sp].count = pr.count[nf];
+        stack[sp].t = near_left ? tr : tl;
+        stack[sp + 1].first = pr.first[nn];
+        stack[sp + 1].count = pr.count[nn];
+        stack[sp + 1].t = near_left ? tl : tr;
+        sp += 2;
+      } else if (hl) {
+        stack[sp].first = pr.first[0];
+        stack[sp].count = pr.count[0];
+        stack[sp].t = tl;
+        sp += 1;
+      } else if (hr) {
+        stack[sp].first = pr.first[1];
+        stack[sp].count = pr.count[1];
+        stack[sp].t = tr;
+        sp += 1;
+      }
+    }
+  }
+  /* intersectAll(planes, r, t_min, limit), geometry.zig:129-139 */
+  for (uint32_t i = 0; i < sc.n_planes; ++i) {
+    double th;
+    if (prim_t(sc.planes[i], o, d, tmin, closest, th)) {
+      closest = th;
+      best_k = -2 - (int32_t)i;
+      if (kAnyHit) { out.t = th; return true; }
+    }
+  }
+  if (best_k == -1) return false;
+  if (!kAnyHit) {
+    if (best_k >= 0) {
+      prim_hit(sc.prims[best_k], o, d, closest, out);
+      out.prim = sc.prim_ids[best_k];
+    } else {
+      const int32_t pi = -2 - best_k;
+      prim_hit(sc.planes[pi], o, d, closest, out);
+      out.prim = (int32_t)sc.n_prims + pi;
+    }
+  }
+  return true;
+}
+
+/* ---------------------------------------------------------- Material ---- */
+/* src/material.zig */
+ZT_D double schlick(double cosine, double eta) { /* material.zig:66-70 */
+  double r0 = (1.0 - eta) / (1.0 + eta);
+  r0 *= r0;
+  return r0 + (1.0 - r0) * zt_pow5(1.0 - cosine);
+}
+
+/* Material.scatter, material.zig:34-62. */
+ZT_D bool material_scatter(const DMat& m, dv3 in_dir, const Hit& h, Rng& rng, dv3& atten, dv3& out_d) {
+  if (m.kind == kLambertian) {
+    dv3 dir = h.normal + rng_unit_vector(rng);
+    if (vnear_zero(dir)) dir = h.normal;
+    atten = L3(m.color);
+    out_d = vnorm(dir);
+    return true;
+  }
+  if (m.kind == kMetal) {
+    dv3 dir = vreflect(vnorm(in_dir), h.normal);
+    if (m.param > 0) dir = vnorm(dir + vscale(rng_unit_vector(rng), m.param));
+    if (vdot(dir, h.normal) <= 0) return false;
+    atten = L3(m.color);
+    out_d = dir;
+    return true;
+  }
+  if (m.kind == kDielectric) {
+    const double eta = h.front_face ? 1.0 / m.param : m.param;
+    const dv3 unit = vnorm(in_dir);
+    const double cos_theta = fmin(vdot(vneg(unit), h.normal), 1.0);
+    const double sin_theta = sqrt(fmax(0.0, 1.0 - cos_theta * cos_theta));
+    const bool cannot_refract = eta * sin_theta > 1.0;
+    /* `or` short-circuits (material.zig:54): no draw under TIR */
+    if (cannot_refract || schlick(cos_theta, eta) > rng_float(rng)) out_d = vreflect(unit, h.normal);
+    else out_d = vrefract(unit, h.normal, eta);
+    atten = V(1, 1, 1);
+    return true;
+  }
+  return false;
+}
+
+/* ------------------------------------------------------------- Light ---- */
+/* src/light.zig */
+ZT_D bool sphere_outside(dv3 center, double radius, dv3 origin) { /* light.zig:47-50 */
+  return vlen(center - origin) > fabs(radius) * (1 + 1e-9);
+}
+
+/* Lights.sample, light.zig:120-166. */
+ZT_D bool lights_sample(const DevScene& sc, dv3 origin, Rng& rng, dv3& odir, double& odist, dv3& orad,
+                        double& opdf) {
+  if (sc.n_lights == 0) return false;
+  /* pick, light.zig:106-115 */
+  const double x = rng_float(rng) * sc.total;
+  uint32_t lo = 0, hi = sc.n_lights - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (sc.cdf[mid] > x) hi = mid;
+    else lo = mid + 1;
+  }
+  const DLight& L = sc.lights[lo];
+  const double select = L.weight / sc.total;
+  if (L.kind == kTriangle) {
+    const dv3 v0 = L3(L.v), v1 = L3(L.v + 3), v2 = L3(L.v + 6);
+    const double su = sqrt(rng_float(rng));
+    const double b2 = rng_float(rng);
+    const dv3 p = (vscale(v0, 1 - su) + vscale(v1, su * (1 - b2))) + vscale(v2, su * b2);
+    const dv3 to = p - origin;
+    const double dist = vlen(to);
+    if (dist < 1e-9) return false;
+    const dv3 dir = vscale(to, 1 / dist);
+    const double cos_l = -vdot(dir, L3(L.normal));
+    if (cos_l <= 1e-9) return false;
+    odir = dir;
+    odist = dist;
+    orad = L3(L.radiance);
+    opdf = select * dist * dist / (cos_l * L.area);
+    return true;
+  }
+  const dv3 center = L3(L.v);
+  const double radius = L.v[3];
+  if (!sphere_outside(center, radius, origin)) return false;
+  const dv3 axis = center - origin;
+  const double d2 = vlen2(axis);
+  const dv3 w = vscale(axis, 1 / sqrt(d2));
+  const double cos_max = sqrt(fmax(0.0, 1 - radius * radius / d2));
+  const double cos_t = 1 - rng_float(rng) * (1 - cos_max);
+  const double sin_t = sqrt(fmax(0.0, 1 - cos_t * cos_t));
+  const double phi = 2 * kPi * rng_float(rng);
+  /* basis, light.zig:53-57 */
+  const dv3 a = fabs(w.x) > 0.9 ? V(0, 1, 0) : V(1, 0, 0);
+  const dv3 bv = vnorm(vcross(w, a));
+  const dv3 bu = vcross(bv, w);
+  double sphi, cphi;
+  zt_sincos(phi, &sphi, &cphi);
+  const dv3 dir = vnorm((vscale(bu, sin_t * cphi) + vscale(bv, sin_t * sphi)) + vscale(w, cos_t));
+  double th;
+  if (!sphere_t(center, radius, origin, dir, 0, INFINITY, th)) return false;
+  /* hit.front_face of the sphere hit at th */
+  const dv3 outward = vdiv((origin + vscale(dir, th)) - center, radius);
+  if (!(vdot(dir, outward) < 0)) return false;
+  odir = dir;
+  odist = th;
+  orad = L3(L.radiance);
+  opdf = select / (2 * kPi * (1 - cos_max));
+  return true;
+}
+
+/* Lights.pdfHit, light.zig:171-198. */
+ZT_D double lights_pdf_hit(const DevScene& sc, dv3 origin, dv3 hit_point) {
+  const dv3 to = hit_point - origin;
+  const double dist = vlen(to);
+  if (dist < 1e-9) return 0;
+  const dv3 dir = vscale(to, 1 / dist);
+  double pdf = 0;
+  for (uint32_t i = 0; i < sc.n_lights; ++i) {
+    const DLight& L = sc.lights[i];
+    const double select = L.weight / sc.total;
+    if (L.kind == kTriangle) {
+      const dv3 v0 = L3(L.v);
+      const dv3 e1 = L3(L.v + 3) - v0, e2 = L3(L.v + 6) - v0;
+      double th;
+      if (!triangle_t(v0, e1, e2, origin, dir, 1e-9, INFINITY, th)) continue;
+      /* Hit.make with the outward normal normalize(e1 x e2) */
+      const dv3 outward = vnorm(vcross(e1, e2));
+      const bool front = vdot(dir, outward) < 0;
+      if (fabs(th - dist) > 1e-6 * dist || !front) continue;
+      const dv3 n = front ? outward : vneg(outward);
+      pdf += select * dist * dist / (-vdot(dir, n) * L.area);
+    } else {
+      const dv3 center = L3(L.v);
+      const double radius = L.v[3];
+      if (!sphere_outside(center, radius, origin)) continue;
+      double th;
+      if (!sphere_t(center, radius, origin, dir, 1e-9, INFINITY, th)) continue;
+      const dv3 outward = vdiv((origin + vscale(dir, th)) - center, radius);
+      const bool front = vdot(dir, outward) < 0;
+      if (fabs(th - dist) > 1e-6 * dist || !front) continue;
+      const double d2 = vlen2(center - origin);
+      const double cos_max = sqrt(fmax(0.0, 1 - radius * radius / d2));
+      pdf += select / (2 * kPi * (1 - cos_max));
+    }
+  }
+  return pdf;
+}
+
+/* ----------------------------------------------------------- Camera ---- */
+ZT_D void camera_ray(const DCamera& c, double s, double t, Rng& rng, dv3& ro, dv3& rd) { /* camera.zig:59-67 */
+  dv3 origin = L3(c.origin);
+  if (c.lens_radius > 0) {
+    const dv3 p = rng_in_unit_disk(rng);
+    const dv3 d = vscale(p, c.lens_radius);
+    origin = (origin + vscale(L3(c.u), d.x)) + vscale(L3(c.v), d.y);
+  }
+  const dv3 target = (L3(c.upper_left) + vscale(L3(c.horizontal), s)) + vscale(L3(c.vertical), t);
+  ro = origin;
+  rd = vnorm(target - origin);
+}
+
+ZT_D dv3 background_radiance(const DBackground& bg, dv3 dir) { /* scene.zig:20-28 */
+  if (bg.kind == 0) return L3(bg.a);
+  const double t = fmax(0.0, fmin(vnorm(dir).y, 1.0));
+  return vlerp(L3(bg.a), L3(bg.b), t);
+}
+
+/* -------------------------------------------------------- Integrator ---- */
+ZT_D double power_weight(double a, double b) { /* render.zig:38-41 */
+  const double a2 = a * a;
+  return a2 / (a2 + b * b);
+}
+
+/* directLight, render.zig:46-56 (shadow ray as an any-hit query). */
+ZT_D dv3 direct_light(const DevScene& sc, dv3 albedo, const Hit& hit, Rng& rng) {
+  dv3 ldir, lrad;
+  double ldist, lpdf;
+  if (!lights_sample(sc, hit.point, rng, ldir, ldist, lrad, lpdf)) return V(0, 0, 0);
+  const double cos_s = vdot(hit.normal, ldir);
+  if (cos_s <= 0 || !(lpdf > 0)) return V(0, 0, 0);
+  Hit sh;
+  if (scene_intersect<true>(sc, hit.point, ldir, kRayEpsilon, ldist * (1 - 1e-6), sh)) return V(0, 0, 0);
+  const double bsdf_pdf = cos_s / kPi;
+  const double scale = cos_s / (kPi * lpdf) * power_weight(lpdf, bsdf_pdf);
+  return vscale(vmul(albedo, lrad), scale);
+}
+
+/* traceWith, render.zig:61-102. */
+struct TraceAux { int32_t first_prim; uint32_t path_len; };
+
+template <bool kAux>
+ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_depth, bool use_nee,
+                    TraceAux* aux) {
+  dv3 radiance = V(0, 0, 0), throughput = V(1, 1, 1);
+  dv3 prev_origin = V(0, 0, 0);
+  double prev_pdf = 0;
+  uint32_t n_ext = 0;
+  if (kAux) aux->first_prim = -1;
+  for (uint64_t depth = 0; depth < max_depth; ++depth) {
+    Hit hit;
+    if (kAux) n_ext++;
+    if (!scene_intersect<false>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
+      if (kAux) aux->path_len = n_ext;
+      return radiance + vmul(throughput, background_radiance(sc.bg, rd));
+    }
+    if (kAux && depth == 0) aux->first_prim = hit.prim;
+    const DMat& mat = sc.mats[hit.material];
+    /* Material.emitted, material.zig:26-32 */
+    const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
+    if (vmaxc(le) > 0) {
+      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, prev_origin, hit.point)) : 1.0;
+      radiance = radiance + vscale(vmul(throughput, le), w);
+    }
+    if (mat.kind == kLambertian && use_nee)
+      radiance = radiance + vmul(throughput, direct_light(sc, L3(mat.color), hit, rng));
+    dv3 atten, sd;
+    if (!material_scatter(mat, rd, hit, rng, atten, sd)) break;
+    throughput = vmul(throughput, atten);
+    prev_pdf = (use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
+    prev_origin = hit.point;
+    ro = hit.point;
+    rd = sd;
+    if (depth + 1 >= kRouletteDepth) {
+      const double p = fmin(vmaxc(throughput), 0.95);
+      if (p <= 0 || rng_float(rng) >= p) break;
+      throughput = vdiv(throughput, p);
+    }
+  }
+  if (kAux) aux->path_len = n_ext;
+  return radiance;
+}
+
+}  // namespace zt
+
+#endif

@@ -1,0 +1,209 @@
+"""Seeded synthetic workloads, built through the public Scene API.
+
+No public benchmark suite or dataset is involved: each workload is generated
+procedurally from a fixed seed, with the shapes, sizes and value
+distributions of the configurations the renderer is measured on.
+
+- ``cornell``: the Cornell box of examples/cornell.txt (five Lambertian
+  walls, a 130x105 one-sided ceiling light of radiance 15, a glass sphere
+  r=90 and a metal sphere with fuzz 0), black background; 256x256, 64 spp,
+  depth 16.
+- ``random_spheres``: ground plane, three r=1 spheres and about 320 r=0.2
+  spheres on a jittered 18x18 grid over [-11, 11]^2 (80% Lambertian with
+  albedo U*U, 15% metal albedo U(0.5,1) fuzz U(0,0.5), 5% glass), sky
+  background, thin lens (aperture 0.1, focus 10); 1280x720, 16 spp, depth 50.
+- ``triangle_heavy``: a 1000x500-cell heightfield (2 triangles per cell,
+  fBm heights) plus 20 icospheres at subdivision 3, Lambertian/metal mix,
+  64 small emissive quads of radiance U(5,20), black background;
+  1920x1080, 64 spp, depth 16.
+"""
+from __future__ import annotations
+
+import math
+from typing import Tuple
+
+import numpy as np
+
+from .api import Background, CameraConfig, Material, Options, Scene, plane, sphere
+
+
+# ------------------------------------------------------------- Cornell ----
+def cornell(metal_fuzz: float = 0.0) -> Scene:
+    """Cornell box, geometry of examples/cornell.txt:15-23."""
+    s = Scene()
+    s.background = Background.solid((0.0, 0.0, 0.0))
+    red = s.add_material(Material.lambertian((0.65, 0.05, 0.05)))
+    green = s.add_material(Material.lambertian((0.12, 0.45, 0.15)))
+    white = s.add_material(Material.lambertian((0.73, 0.73, 0.73)))
+    light = s.add_material(Material.emissive((15.0, 15.0, 15.0)))
+    glass = s.add_material(Material.dielectric(1.5))
+    steel = s.add_material(Material.metal((0.85, 0.85, 0.88), metal_fuzz))
+    s.add_quad((555, 0, 0), (0, 555, 0), (0, 0, 555), red)
+    s.add_quad((0, 0, 0), (0, 555, 0), (0, 0, 555), green)
+    s.add_quad((343, 554, 332), (-130, 0, 0), (0, 0, -105), light)  # faces down
+    s.add_quad((0, 0, 0), (555, 0, 0), (0, 0, 555), white)  # floor
+    s.add_quad((555, 555, 555), (-555, 0, 0), (0, 0, -555), white)  # ceiling
+    s.add_quad((0, 0, 555), (555, 0, 0), (0, 555, 0), white)  # back wall
+    s.add(sphere((190, 90, 190), 90, glass))
+    s.add(sphere((380, 120, 360), 120, steel))
+    s.camera = CameraConfig(look_from=(278, 278, -800), look_at=(278, 278, 0), vfov=40)
+    return s
+
+
+CORNELL_OPTIONS = Options(width=256, height=256, spp=64, max_depth=16, seed=0)
+
+
+# ------------------------------------------------------ random spheres ----
+def random_spheres(seed: int = 0, grid: int = 18, extent: float = 11.0) -> Scene:
+    """Ground plane + 3 big spheres + jittered grid of r=0.2 spheres."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    s.background = Background.sky((1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
+    ground = s.add_material(Material.lambertian((0.5, 0.5, 0.5)))
+    s.add(plane((0.0, 0.0, 0.0), (0.0, 1.0, 0.0), ground))
+    glass = s.add_material(Material.dielectric(1.5))
+    brown = s.add_material(Material.lambertian((0.4, 0.2, 0.1)))
+    polished = s.add_material(Material.metal((0.7, 0.6, 0.5), 0.0))
+    big = [((0.0, 1.0, 0.0), glass), ((-4.0, 1.0, 0.0), brown), ((4.0, 1.0, 0.0), polished)]
+    for c, m in big:
+        s.add(sphere(c, 1.0, m))
+    cell = 2.0 * extent / grid
+    for i in range(grid):
+        for j in range(grid):
+            jx, jz, choose = rng.random(), rng.random(), rng.random()
+            cx = -extent + (i + 0.05 + 0.9 * jx) * cell
+            cz = -extent + (j + 0.05 + 0.9 * jz) * cell
+            if any(math.hypot(cx - c[0], cz - c[2]) < 1.2 for c, _ in big):
+                continue
+            if choose < 0.8:
+                albedo = tuple(float(a) for a in rng.random(3) * rng.random(3))
+                m = s.add_material(Material.lambertian(albedo))
+            elif choose < 0.95:
+                albedo = tuple(float(a) for a in rng.uniform(0.5, 1.0, 3))
+                m = s.add_material(Material.metal(albedo, float(rng.uniform(0.0, 0.5))))
+            else:
+                m = glass
+            s.add(sphere((cx, 0.2, cz), 0.2, m))
+    s.camera = CameraConfig(look_from=(13, 2, 3), look_at=(0, 0, 0), vfov=20, aperture=0.1, focus_dist=10.0)
+    return s
+
+
+SPHERES_OPTIONS = Options(width=1280, height=720, spp=16, max_depth=50, seed=0)
+
+
+# ------------------------------------------------------ triangle heavy ----
+def _value_noise(x: np.ndarray, z: np.ndarray, rng: np.random.Generator, freq: float) -> np.ndarray:
+    """Smoothly interpolated lattice noise in [-1, 1]."""
+    n = int(math.ceil(freq)) + 2
+    lattice = rng.uniform(-1.0, 1.0, (n + 1, n + 1))
+    gx, gz = x * freq, z * freq
+    ix, iz = np.floor(gx).astype(np.int64), np.floor(gz).astype(np.int64)
+    fx, fz = gx - ix, gz - iz
+    sx, sz = fx * fx * (3 - 2 * fx), fz * fz * (3 - 2 * fz)
+    ix %= n
+    iz %= n
+    a = lattice[ix, iz] * (1 - sx) + lattice[ix + 1, iz] * sx
+    b = lattice[ix, iz + 1] * (1 - sx) + lattice[ix + 1, iz + 1] * sx
+    return a * (1 - sz) + b * sz
+
+
+def heightfield(nx: int, nz: int, size_x: float, size_z: float, seed: int, octaves: int = 6,
+                amplitude: float = 3.0) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """(nx+1)x(nz+1) vertex grid with fBm heights; returns triangle corner
+    arrays v0, v1, v2 (2 per cell, front face up)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(-size_x / 2, size_x / 2, nx + 1)
+    zs = np.linspace(-size_z / 2, size_z / 2, nz + 1)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    u, v = (X - xs[0]) / size_x, (Z - zs[0]) / size_z
+    H = np.zeros_like(X)
+    amp, freq = amplitude, 4.0
+    for _ in range(octaves):
+        H += amp * _value_noise(u, v, rng, freq)
+        amp *= 0.5
+        freq *= 2.0
+    P = np.stack([X, H, Z], axis=-1)
+    p00, p10 = P[:-1, :-1].reshape(-1, 3), P[1:, :-1].reshape(-1, 3)
+    p01, p11 = P[:-1, 1:].reshape(-1, 3), P[1:, 1:].reshape(-1, 3)
+    v0 = np.concatenate([p00, p00])
+    v1 = np.concatenate([p01, p11])
+    v2 = np.concatenate([p11, p10])
+    return v0, v1, v2, H
+
+
+def icosphere(subdivisions: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere: (vertices, faces) with outward (counter-clockwise)
+    winding; 20 * 4^subdivisions faces."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [tuple(c / math.sqrt(1 + t * t) for c in v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+        new_faces = []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = np.add(verts[a], verts[b]) / 2.0
+                m = m / np.linalg.norm(m)
+                verts.append(tuple(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            new_faces += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = new_faces
+    return np.array(verts, np.float64), np.array(faces, np.int64)
+
+
+def triangle_heavy(seed: int = 0, nx: int = 1000, nz: int = 500, n_ico: int = 20, ico_subdiv: int = 3,
+                   n_lights: int = 64) -> Scene:
+    """Heightfield + icospheres + small emissive quads, black background."""
+    rng = np.random.default_rng(seed + 1000)
+    size_x, size_z = 100.0, 50.0
+    s = Scene()
+    s.background = Background.solid((0.0, 0.0, 0.0))
+    terrain = s.add_material(Material.lambertian((0.45, 0.5, 0.4)))
+    v0, v1, v2, H = heightfield(nx, nz, size_x, size_z, seed)
+    s.add_triangles(v0, v1, v2, terrain)
+
+    def height_at(x, z):
+        i = int(round((x + size_x / 2) / size_x * nx))
+        j = int(round((z + size_z / 2) / size_z * nz))
+        return float(H[min(max(i, 0), nx), min(max(j, 0), nz)])
+
+    verts, faces = icosphere(ico_subdiv)
+    for k in range(n_ico):
+        cx, cz = rng.uniform(-0.4 * size_x, 0.4 * size_x), rng.uniform(-0.4 * size_z, 0.4 * size_z)
+        r = rng.uniform(1.0, 3.0)
+        cy = height_at(cx, cz) + r * 0.8
+        if rng.random() < 0.5:
+            m = s.add_material(Material.lambertian(tuple(float(a) for a in rng.uniform(0.2, 0.9, 3))))
+        else:
+            m = s.add_material(Material.metal(tuple(float(a) for a in rng.uniform(0.5, 1.0, 3)),
+                                              float(rng.uniform(0.0, 0.3))))
+        P = verts * r + np.array([cx, cy, cz])
+        s.add_triangles(P[faces[:, 0]], P[faces[:, 1]], P[faces[:, 2]], m)
+    for k in range(n_lights):
+        cx, cz = rng.uniform(-0.45 * size_x, 0.45 * size_x), rng.uniform(-0.45 * size_z, 0.45 * size_z)
+        y = height_at(cx, cz) + rng.uniform(4.0, 8.0)
+        m = s.add_material(Material.emissive(tuple([float(rng.uniform(5.0, 20.0))] * 3)))
+        w = rng.uniform(0.6, 1.5)
+        # corner, u, v with u x v pointing down (-y): faces the terrain
+        s.add_quad((cx - w / 2, y, cz - w / 2), (w, 0, 0), (0, 0, w), m)
+    s.camera = CameraConfig(look_from=(0.0, 22.0, 48.0), look_at=(0.0, 0.0, 0.0), vfov=55)
+    return s
+
+
+TRIANGLE_HEAVY_OPTIONS = Options(width=1920, height=1080, spp=64, max_depth=16, seed=0)
+
+WORKLOADS = {
+    "cornell": (cornell, CORNELL_OPTIONS),
+    "random_spheres": (random_spheres, SPHERES_OPTIONS),
+    "triangle_heavy": (triangle_heavy, TRIANGLE_HEAVY_OPTIONS),
+}

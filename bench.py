@@ -46,6 +46,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
+    p.add_argument("--capacity", type=int, default=0, help="zt_gpu_config.queue_capacity (wavefront)")
     return p.parse_args()
 
 
@@ -197,7 +198,7 @@ def b200_arm(args):
     scene.build()
     counts = scene.counts()
     scene.upload()
-    gcfg = zt.GpuConfig(mode=args.mode)
+    gcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity)
     npix = o.width * o.height
     samples = npix * o.spp
     out = torch.empty(npix * 3, dtype=torch.float64, device="cuda")

@@ -34,12 +34,15 @@ class OracleBackend:
 class GpuBackend:
     name = "gpu"
 
+    def __init__(self, mode: int = zt.MODE_MEGAKERNEL):
+        self.mode = mode
+
     def render(self, scene: zt.Scene, width, height, spp, max_depth, threads=1, seed=0, tile_size=16,
                light_sampling=True) -> np.ndarray:
         scene.build()
         opts = zt.Options(width=width, height=height, spp=spp, max_depth=max_depth, threads=threads, seed=seed,
                           tile_size=tile_size, light_sampling=light_sampling)
-        return zt.render(scene, opts).pixels
+        return zt.render(scene, opts, zt.GpuConfig(mode=self.mode)).pixels
 
     def mean_radiance(self, scene: zt.Scene, origin, direction, seed, n, max_depth, nee) -> np.ndarray:
         scene.build()

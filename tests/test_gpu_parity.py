@@ -16,6 +16,7 @@ import zigtrace_b200 as zt
 from zigtrace_b200 import scenes
 
 pytestmark = pytest.mark.gpu
+MODES = [pytest.param(zt.MODE_MEGAKERNEL, id="mega"), pytest.param(zt.MODE_WAVEFRONT, id="wavefront")]
 
 DEBUG_CASES = {
     "demo": (K.demo_scene, dict(width=48, height=32, max_depth=8)),
@@ -34,6 +35,8 @@ def test_first_hit_ids_and_path_lengths_bit_exact(name):
     scene = build()
     if name == "coincident":
         scene.camera = zt.CameraConfig(look_from=(0, 0, 30), look_at=(0, 0, 0), vfov=50)
+    if name == "lamps":
+        scene.camera = zt.CameraConfig(look_from=(0, 2.5, 8), look_at=(0, 1.5, 0), vfov=50)
     scene.build()
     fp, pl = zt.render_debug(scene, zt.Options(o["width"], o["height"], 1, o["max_depth"]))
     ofp, opl = O.OracleScene.from_scene(scene).render_debug(o["width"], o["height"], o["max_depth"])
@@ -48,25 +51,27 @@ def test_rng_streams_bit_exact_many_pixels():
         assert [int(x) for x in got[i]] == [int(x) for x in O.Rng.for_stream(12345, i).next_n(4)]
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("spp,light_sampling", [(4, True), (4, False)])
-def test_cornell_small_bit_exact(spp, light_sampling):
+def test_cornell_small_bit_exact(spp, light_sampling, mode):
     scene = scenes.cornell().build()
-    img = zt.render(scene, zt.Options(64, 64, spp, 16, light_sampling=light_sampling)).pixels
+    img = zt.render(scene, zt.Options(64, 64, spp, 16, light_sampling=light_sampling), zt.GpuConfig(mode)).pixels
     want = O.OracleScene.from_scene(scene).render(64, 64, spp, 16, light_sampling=light_sampling)
     assert img.tobytes() == want.tobytes()
 
 
-def test_cornell_full_size_bit_exact():
+@pytest.mark.parametrize("mode", MODES)
+def test_cornell_full_size_bit_exact(mode):
     """The Cornell workload at its full size: 256x256, 64 spp, depth 16."""
     scene = scenes.cornell().build()
     o = scenes.CORNELL_OPTIONS
-    img = zt.render(scene, o).pixels
+    img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
     want = O.OracleScene.from_scene(scene).render(o.width, o.height, o.spp, o.max_depth)
     assert img.tobytes() == want.tobytes()
 
 
-def _subset_check(scene, o: zt.Options, n_pixels: int, seed: int = 0):
-    img = zt.render(scene, o).pixels
+def _subset_check(scene, o: zt.Options, n_pixels: int, mode: int, seed: int = 0):
+    img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
     rng = np.random.default_rng(seed)
     pix = np.unique(rng.integers(0, o.width * o.height, n_pixels)).astype(np.uint64)
     want = O.OracleScene.from_scene(scene).render_pixels(o.width, o.height, o.spp, o.max_depth, pix, seed=o.seed,
@@ -76,49 +81,58 @@ def _subset_check(scene, o: zt.Options, n_pixels: int, seed: int = 0):
     return img
 
 
-def test_random_spheres_full_size_subset_bit_exact():
+@pytest.mark.parametrize("mode", MODES)
+def test_random_spheres_full_size_subset_bit_exact(mode):
     """1280x720, 16 spp, depth 50; 3000 random pixels re-rendered by the oracle."""
     scene = scenes.random_spheres().build()
-    img = _subset_check(scene, scenes.SPHERES_OPTIONS, 3000)
+    img = _subset_check(scene, scenes.SPHERES_OPTIONS, 3000, mode)
     assert img.mean() > 0.1
 
 
-def test_triangle_heavy_subset_bit_exact():
+@pytest.mark.parametrize("mode", MODES)
+def test_triangle_heavy_subset_bit_exact(mode):
     """The 1M-triangle scene at full resolution, 4 spp; 400 oracle pixels."""
     scene = scenes.triangle_heavy().build()
     o = zt.Options(1920, 1080, 4, 16)
-    _subset_check(scene, o, 400)
+    _subset_check(scene, o, 400, mode)
 
 
-def test_render_is_deterministic_and_seed_dependent():
+@pytest.mark.parametrize("mode", MODES)
+def test_render_is_deterministic_and_seed_dependent(mode):
     scene = scenes.random_spheres().build()
     o = zt.Options(320, 180, 4, 50, seed=7)
-    a = zt.render(scene, o).pixels
-    b = zt.render(scene, o).pixels
+    g = zt.GpuConfig(mode)
+    a = zt.render(scene, o, g).pixels
+    b = zt.render(scene, o, g).pixels
     assert a.tobytes() == b.tobytes()
-    c = zt.render(scene, zt.Options(320, 180, 4, 50, seed=8)).pixels
+    c = zt.render(scene, zt.Options(320, 180, 4, 50, seed=8), g).pixels
     assert a.tobytes() != c.tobytes()
 
 
-def test_render_device_on_torch_stream_matches_host_render():
+@pytest.mark.parametrize("mode", MODES)
+def test_render_device_on_torch_stream_matches_host_render(mode):
     import torch
     scene = scenes.cornell().build()
     o = zt.Options(96, 64, 2, 16)
     want = zt.render(scene, o).pixels
     scene.upload()
     out = torch.empty(96 * 64 * 3, dtype=torch.float64, device="cuda")
-    zt.render_device(scene, o, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):  # the second launch reuses the cached graph
+        out.fill_(-1.0)
+        zt.render_device(scene, o, out.data_ptr(), torch.cuda.current_stream().cuda_stream, zt.GpuConfig(mode))
     torch.cuda.synchronize()
     assert out.cpu().numpy().reshape(-1, 3).tobytes() == want.tobytes()
 
 
-def test_edge_options():
+@pytest.mark.parametrize("mode", MODES)
+def test_edge_options(mode):
     scene = K.demo_scene().build()
-    assert (zt.render(scene, zt.Options(5, 3, 2, 0)).pixels == 0).all()  # max_depth 0: loop never runs
-    one = zt.render(scene, zt.Options(1, 1, 3, 8)).pixels
+    g = zt.GpuConfig(mode)
+    assert (zt.render(scene, zt.Options(5, 3, 2, 0), g).pixels == 0).all()  # max_depth 0: loop never runs
+    one = zt.render(scene, zt.Options(1, 1, 3, 8), g).pixels
     want = O.OracleScene.from_scene(scene).render(1, 1, 3, 8)
     assert one.tobytes() == want.tobytes()
-    odd = zt.render(scene, zt.Options(37, 23, 3, 8, seed=2**64 - 1)).pixels
+    odd = zt.render(scene, zt.Options(37, 23, 3, 8, seed=2**64 - 1), g).pixels
     want = O.OracleScene.from_scene(scene).render(37, 23, 3, 8, seed=2**64 - 1)
     assert odd.tobytes() == want.tobytes()
     with pytest.raises(zt.ZigtraceError) as ei:

@@ -8,7 +8,11 @@ import pytest
 import kat_scenes as K
 from backends import GpuBackend, OracleBackend
 
-BACKENDS = [pytest.param(OracleBackend(), id="oracle"), pytest.param(GpuBackend(), id="gpu", marks=pytest.mark.gpu)]
+import zigtrace_b200 as zt
+
+BACKENDS = [pytest.param(OracleBackend(), id="oracle"),
+            pytest.param(GpuBackend(zt.MODE_MEGAKERNEL), id="gpu-mega", marks=pytest.mark.gpu),
+            pytest.param(GpuBackend(zt.MODE_WAVEFRONT), id="gpu-wavefront", marks=pytest.mark.gpu)]
 
 
 @pytest.mark.parametrize("be", BACKENDS)

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "scene_host.h"
+#include "wavefront.cuh"
 #include "zt_device.cuh"
 
 using namespace zt;
@@ -31,11 +32,25 @@ struct zt_host_staging {
   DevScene view;  /* counts, root, total; pointers unset */
 };
 
+/* Wavefront path state (grow-only) and the cached executable graph that
+ * drives it.  The graph bakes its kernel arguments in, so it is reused only
+ * for an identical launch (same scene view, parameters and output). */
+struct zt_wavefront_cache {
+  void* block = nullptr;
+  size_t bytes = 0;
+  uint32_t capacity = 0;
+  zt::WfState state;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;  /* recorded after the last launch of exec */
+  unsigned char key[sizeof(zt::DevScene) + sizeof(zt::RenderParams) + 2 * sizeof(void*)] = {};
+};
+
 struct zt_device_buffers {
   int device = -1;
   void* block = nullptr;           /* all scene arrays */
   unsigned int* counter = nullptr; /* work counter of the persistent grid */
   DevScene view;
+  zt_wavefront_cache wf;
 };
 
 namespace zt {
@@ -57,6 +72,10 @@ void release_device(zt_scene* s) {
   int cur = -1;
   cudaGetDevice(&cur);
   if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
+  if (d->wf.done) cudaEventSynchronize(d->wf.done);
+  if (d->wf.exec) cudaGraphExecDestroy(d->wf.exec);
+  if (d->wf.done) cudaEventDestroy(d->wf.done);
+  cudaFree(d->wf.block);
   cudaFree(d->block);
   cudaFree(d->counter);
   if (d->device >= 0 && d->device != cur) cudaSetDevice(cur);
@@ -214,17 +233,20 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
 /* Persistent megakernel: each warp takes 32 consecutive pixels from the
  * device work counter until the image is exhausted (the device form of
  * Context.work's atomic tile counter, render.zig:113-119). */
-__global__ void __launch_bounds__(128) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
+/* 7 blocks of 128 per SM (<= 73 registers): measured fastest on the
+ * 1M-triangle workload among 4..8 blocks per SM. */
+__global__ void __launch_bounds__(128, 7) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
                                                      unsigned int* __restrict__ counter) {
-  const uint64_t npix = p.width * p.height;
+  /* A warp renders an 8x4 pixel tile, so its camera rays are coherent. */
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
-    unsigned base = 0;
-    if (lane == 0) base = atomicAdd(counter, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if ((uint64_t)base >= npix) return;
-    const uint64_t pix = (uint64_t)base + lane;
-    if (pix < npix) render_pixel<false>(sc, p, pix, out, nullptr);
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= tiles) return;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    if (x < p.width && y < p.height) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
   }
 }
 
@@ -244,6 +266,172 @@ __global__ void k_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_stream
   if (i >= n_streams) return;
   Rng r = rng_for_stream(seed, stream0 + i);
   for (uint64_t k = 0; k < n_draws; ++k) out[i * n_draws + k] = rng_next(r);
+}
+
+/* ------------------------------------------------------------ Wavefront ---- */
+
+/* Slots 0..n0-1 start pixels 0..n0-1 (render.zig:135-140). */
+__global__ void k_wf_init(RenderParams p, WfState w, uint32_t n0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    w.ctl[kCtlIter] = 0;
+    w.ctl[kCtlExt0] = n0;
+    w.ctl[kCtlExt0 + 1] = 0;
+    w.ctl[kCtlShadow] = 0;
+    w.ctl[kCtlNextPixel] = n0;
+    w.ctl[kCtlError] = 0;
+  }
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n0; s += gridDim.x * blockDim.x) {
+    Rng rng;
+    start_pixel(w, p, s, s, rng);
+    start_sample(w, p, s, rng);
+    st_rng(w, s, rng);
+    w.queue[0][s] = s;
+  }
+}
+
+/* Closest hit of every queued ray (scene.zig:108-116). */
+__global__ void __launch_bounds__(128) k_wf_extend(DevScene sc, WfState w) {
+  const uint32_t cur = w.ctl[kCtlIter] & 1;
+  const uint32_t n = w.ctl[kCtlExt0 + cur];
+  const uint32_t* __restrict__ q = w.queue[cur];
+  const uint32_t c = w.capacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = q[i];
+    double t;
+    const int32_t k = scene_query<false>(sc, ld3(w.ray, c, s, 0), ld3(w.ray, c, s, 3), kRayEpsilon, INFINITY, t);
+    w.hit_t[s] = t;
+    w.hit_k[s] = k;
+  }
+}
+
+/* One bounce of traceWith after the intersection (render.zig:73-99); the
+ * light sample's visibility is left to k_wf_shadow. */
+__global__ void __launch_bounds__(128) k_wf_shade(DevScene sc, RenderParams p, WfState w, double* __restrict__ out) {
+  const uint32_t it = w.ctl[kCtlIter];
+  const uint32_t cur = it & 1, nxt = cur ^ 1;
+  const uint32_t n = w.ctl[kCtlExt0 + cur];
+  const uint32_t* __restrict__ q = w.queue[cur];
+  uint32_t* qn = w.queue[nxt];
+  uint32_t* nn = &w.ctl[kCtlExt0 + nxt];
+  const uint32_t c = w.capacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = q[i];
+    Rng rng = ld_rng(w, s);
+    const dv3 o = ld3(w.ray, c, s, 0), d = ld3(w.ray, c, s, 3);
+    dv3 tp = ld3(w.tp, c, s, 0);
+    dv3 rad = ld3(w.rad, c, s, 0);
+    const int32_t k = w.hit_k[s];
+    if (k == -1) { /* miss: background, render.zig:73-75 */
+      rad = rad + vmul(tp, background_radiance(sc.bg, d));
+      st3(w.rad, c, s, 0, rad);
+      finish_sample(w, p, s, rng, out, qn, nn);
+      continue;
+    }
+    Hit hit;
+    hit_from(sc, k, o, d, w.hit_t[s], hit);
+    const DMat& mat = sc.mats[hit.material];
+    const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
+    if (vmaxc(le) > 0) {
+      const double prev_pdf = w.prev[3 * (size_t)c + s];
+      const double wt =
+          prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, ld3(w.prev, c, s, 0), hit.point)) : 1.0;
+      rad = rad + vscale(vmul(tp, le), wt);
+    }
+    bool pending = false;
+    if (mat.kind == kLambertian && p.use_nee) { /* directLight, render.zig:46-56 */
+      dv3 ldir, lrad;
+      double ldist, lpdf;
+      if (lights_sample(sc, hit.point, rng, ldir, ldist, lrad, lpdf)) {
+        const double cos_s = vdot(hit.normal, ldir);
+        if (!(cos_s <= 0 || !(lpdf > 0))) {
+          const double bsdf_pdf = cos_s / kPi;
+          const double scale = cos_s / (kPi * lpdf) * power_weight(lpdf, bsdf_pdf);
+          const dv3 direct = vscale(vmul(L3(mat.color), lrad), scale);
+          double* nee = w.nee;
+          st3(nee, c, s, 0, hit.point);
+          st3(nee, c, s, 3, ldir);
+          nee[6 * (size_t)c + s] = ldist * (1 - 1e-6);
+          st3(nee, c, s, 7, direct);
+          st3(nee, c, s, 10, tp);
+          pending = true;
+        }
+      }
+      if (!pending) rad = rad + vmul(tp, V(0, 0, 0)); /* directLight returned zero */
+    }
+    dv3 atten, sd;
+    bool alive = material_scatter(mat, d, hit, rng, atten, sd);
+    uint32_t depth = w.depth[s];
+    if (alive) {
+      tp = vmul(tp, atten);
+      const double prev_pdf = (p.use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
+      st3(w.prev, c, s, 0, hit.point);
+      w.prev[3 * (size_t)c + s] = prev_pdf;
+      st3(w.ray, c, s, 0, hit.point);
+      st3(w.ray, c, s, 3, sd);
+      if (depth + 1 >= kRouletteDepth) { /* render.zig:94-99 */
+        const double pr = fmin(vmaxc(tp), 0.95);
+        if (pr <= 0 || rng_float(rng) >= pr) alive = false;
+        else tp = vdiv(tp, pr);
+      }
+      depth += 1;
+      if (alive && (uint64_t)depth >= p.max_depth) alive = false; /* loop condition, render.zig:72 */
+      st3(w.tp, c, s, 0, tp);
+      w.depth[s] = depth;
+    }
+    st3(w.rad, c, s, 0, rad);
+    st_rng(w, s, rng);
+    if (pending) {
+      w.flags[s] = alive ? 0u : 1u;
+      push(w.shadow_q, &w.ctl[kCtlShadow], s);
+      if (alive) push(qn, nn, s);
+    } else if (alive) {
+      push(qn, nn, s);
+    } else {
+      finish_sample(w, p, s, rng, out, qn, nn);
+    }
+  }
+}
+
+/* Visibility of the light samples (render.zig:50-51) and the deferred NEE
+ * add; finishes paths that ended with a sample pending. */
+__global__ void __launch_bounds__(128) k_wf_shadow(DevScene sc, RenderParams p, WfState w, double* __restrict__ out) {
+  const uint32_t nxt = (w.ctl[kCtlIter] & 1) ^ 1;
+  const uint32_t n = w.ctl[kCtlShadow];
+  uint32_t* qn = w.queue[nxt];
+  uint32_t* nn = &w.ctl[kCtlExt0 + nxt];
+  const uint32_t c = w.capacity;
+  const double* __restrict__ nee = w.nee;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = w.shadow_q[i];
+    double t;
+    const bool occluded = scene_query<true>(sc, ld3(nee, c, s, 0), ld3(nee, c, s, 3), kRayEpsilon,
+                                            nee[6 * (size_t)c + s], t) != -1;
+    const dv3 direct = occluded ? V(0, 0, 0) : ld3(nee, c, s, 7);
+    const dv3 rad = ld3(w.rad, c, s, 0) + vmul(ld3(nee, c, s, 10), direct);
+    st3(w.rad, c, s, 0, rad);
+    if (w.flags[s] & 1u) {
+      Rng rng = ld_rng(w, s);
+      finish_sample(w, p, s, rng, out, qn, nn);
+    }
+  }
+}
+
+/* Swaps the queues and sets the while-node condition.  The loop provably
+ * ends (every active slot advances one bounce per iteration); max_iter is a
+ * guard that reports an error instead of looping. */
+__global__ void k_wf_advance(WfState w, cudaGraphConditionalHandle h, uint64_t max_iter) {
+  const uint32_t it = w.ctl[kCtlIter];
+  const uint32_t nxt = (it & 1) ^ 1;
+  const uint32_t n_next = w.ctl[kCtlExt0 + nxt];
+  w.ctl[kCtlExt0 + (it & 1)] = 0;
+  w.ctl[kCtlShadow] = 0;
+  w.ctl[kCtlIter] = it + 1;
+  bool go = n_next > 0;
+  if (go && (uint64_t)it + 1 >= max_iter) {
+    w.ctl[kCtlError] = 1;
+    go = false;
+  }
+  cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
 /* meanRadiance's loop (render.zig:290-302): one thread, one RNG stream, n
@@ -276,21 +464,159 @@ static int sm_count() {
   return cached;
 }
 
+template <typename K>
+static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  uint64_t blocks = (uint64_t)sm_count() * per_sm;
+  const uint64_t need = (work_items + block - 1) / block;
+  if (blocks > need) blocks = need;
+  return (unsigned)(blocks > 0 ? blocks : 1);
+}
+
+static zt_status launch_mega(zt_scene* s, const RenderParams& p, double* d_out, cudaStream_t stream) {
+  zt_device_buffers* d = s->device;
+  ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
+  const unsigned blocks = persistent_grid(k_render_mega, 128, p.width * p.height);
+  k_render_mega<<<blocks, 128, 0, stream>>>(launch_view(s), p, d_out, d->counter);
+  ZT_CUDA(cudaGetLastError(), "launch k_render_mega");
+  return ZT_OK;
+}
+
+/* Carves the wavefront arrays out of one allocation of `cap` slots. */
+static zt_status wavefront_state(zt_device_buffers* d, uint32_t cap) {
+  zt_wavefront_cache& c = d->wf;
+  if (c.block && c.capacity >= cap) return ZT_OK;
+  if (c.done) cudaEventSynchronize(c.done);
+  if (c.exec) { cudaGraphExecDestroy(c.exec); c.exec = nullptr; }
+  cudaFree(c.block);
+  c.block = nullptr;
+  c.capacity = 0;
+  const size_t n = cap;
+  const size_t sizes[] = {4 * n, 4 * n, 4 * n, 4 * n, 32 * n, 48 * n, 24 * n, 24 * n, 24 * n, 32 * n,
+                          8 * n, 4 * n, 104 * n, 4 * n, 4 * n, 4 * n, 64};
+  size_t offs[17], cur = 0;
+  for (int i = 0; i < 17; ++i) { offs[i] = cur; cur = align256(cur + sizes[i]); }
+  ZT_CUDA(cudaMalloc(&c.block, cur), "allocate wavefront state");
+  char* b = (char*)c.block;
+  WfState& w = c.state;
+  w.pix = (uint32_t*)(b + offs[0]);
+  w.sample = (uint32_t*)(b + offs[1]);
+  w.depth = (uint32_t*)(b + offs[2]);
+  w.flags = (uint32_t*)(b + offs[3]);
+  w.rng = (uint64_t*)(b + offs[4]);
+  w.ray = (double*)(b + offs[5]);
+  w.tp = (double*)(b + offs[6]);
+  w.rad = (double*)(b + offs[7]);
+  w.sum = (double*)(b + offs[8]);
+  w.prev = (double*)(b + offs[9]);
+  w.hit_t = (double*)(b + offs[10]);
+  w.hit_k = (int32_t*)(b + offs[11]);
+  w.nee = (double*)(b + offs[12]);
+  w.queue[0] = (uint32_t*)(b + offs[13]);
+  w.queue[1] = (uint32_t*)(b + offs[14]);
+  w.shadow_q = (uint32_t*)(b + offs[15]);
+  w.ctl = (uint32_t*)(b + offs[16]);
+  w.capacity = cap;
+  c.bytes = cur;
+  c.capacity = cap;
+  return ZT_OK;
+}
+
+/* Builds the executable graph: while (queue not empty) { extend; shade;
+ * shadow; advance }.  The loop runs on the device; the host never waits. */
+static zt_status build_wavefront_graph(const DevScene& view, const RenderParams& p, const WfState& w, double* d_out,
+                                       cudaGraphExec_t* exec_out) {
+  cudaGraph_t g = nullptr;
+  cudaStream_t cs = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  cudaGraphConditionalHandle h;
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const uint64_t cap = w.capacity;
+      k_wf_extend<<<persistent_grid(k_wf_extend, 128, cap), 128, 0, cs>>>(view, w);
+      k_wf_shade<<<persistent_grid(k_wf_shade, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
+      k_wf_shadow<<<persistent_grid(k_wf_shadow, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
+      /* every iteration advances each active slot by one bounce: a bound */
+      const double bound = (double)(p.width * p.height) * (double)p.spp * (double)(p.max_depth + 1) + 16.0;
+      const uint64_t max_iter = bound > 4.0e9 ? 4000000000ull : (uint64_t)bound;
+      k_wf_advance<<<1, 1, 0, cs>>>(w, h, max_iter);
+      cudaGraph_t captured = nullptr;
+      cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
+      e = e2 != cudaSuccess ? e2 : cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+  if (cs) cudaStreamDestroy(cs);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "build wavefront graph");
+  *exec_out = exec;
+  return ZT_OK;
+}
+
+static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t capacity, double* d_out,
+                                  cudaStream_t stream) {
+  zt_device_buffers* d = s->device;
+  const uint64_t npix = p.width * p.height;
+  const uint32_t cap = (uint32_t)(capacity && capacity < npix ? capacity : (npix < (1u << 22) ? npix : (1u << 22)));
+  zt_status rc = wavefront_state(d, cap);
+  if (rc != ZT_OK) return rc;
+  zt_wavefront_cache& c = d->wf;
+  const DevScene view = launch_view(s);
+  unsigned char key[sizeof c.key];
+  memset(key, 0, sizeof key);
+  memcpy(key, &view, sizeof view);
+  memcpy(key + sizeof view, &p, sizeof p);
+  memcpy(key + sizeof view + sizeof p, &d_out, sizeof d_out);
+  const uint64_t capk = cap;
+  memcpy(key + sizeof view + sizeof p + sizeof d_out, &capk, sizeof(void*));
+  if (!c.exec || memcmp(key, c.key, sizeof key) != 0) {
+    if (c.done) cudaEventSynchronize(c.done);
+    if (c.exec) { cudaGraphExecDestroy(c.exec); c.exec = nullptr; }
+    rc = build_wavefront_graph(view, p, c.state, d_out, &c.exec);
+    if (rc != ZT_OK) return rc;
+    memcpy(c.key, key, sizeof key);
+    if (!c.done) ZT_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "create event");
+  }
+  const uint32_t n0 = (uint32_t)(npix < cap ? npix : cap);
+  k_wf_init<<<persistent_grid(k_wf_init, 256, n0), 256, 0, stream>>>(p, c.state, n0);
+  ZT_CUDA(cudaGetLastError(), "launch k_wf_init");
+  ZT_CUDA(cudaGraphLaunch(c.exec, stream), "launch wavefront graph");
+  ZT_CUDA(cudaEventRecord(c.done, stream), "record event");
+  return ZT_OK;
+}
+
 static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* d_out,
                                cudaStream_t stream) {
-  (void)cfg;
-  zt_device_buffers* d = s->device;
   const RenderParams p = make_params(s, o);
-  ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
-  int per_sm = 0;
-  ZT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_mega, 128, 0), "occupancy query");
-  if (per_sm < 1) per_sm = 1;
-  const uint64_t npix = o->width * o->height;
-  uint64_t blocks = (uint64_t)sm_count() * per_sm;
-  const uint64_t need = (npix + 127) / 128;
-  if (blocks > need) blocks = need;
-  k_render_mega<<<(unsigned)blocks, 128, 0, stream>>>(launch_view(s), p, d_out, d->counter);
-  ZT_CUDA(cudaGetLastError(), "launch k_render_mega");
+  if (p.max_depth == 0) { /* traceWith never enters its loop: every sample is zero */
+    ZT_CUDA(cudaMemsetAsync(d_out, 0, p.width * p.height * 3 * sizeof(double), stream), "clear framebuffer");
+    return ZT_OK;
+  }
+  const uint32_t mode = cfg ? cfg->mode : ZT_MODE_AUTO;
+  if (mode == ZT_MODE_WAVEFRONT) return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
+  if (mode > ZT_MODE_WAVEFRONT) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
+  return launch_mega(s, p, d_out, stream);
+}
+
+/* Error word of the last wavefront launch (after the stream is idle). */
+static zt_status wavefront_status(zt_scene* s, const zt_gpu_config* cfg) {
+  if (!cfg || cfg->mode != ZT_MODE_WAVEFRONT || !s->device || !s->device->wf.block) return ZT_OK;
+  uint32_t err = 0;
+  ZT_CUDA(cudaMemcpy(&err, s->device->wf.state.ctl + kCtlError, sizeof err, cudaMemcpyDeviceToHost), "read status");
+  if (err) return fail(ZT_ERR_TIMEOUT, "wavefront loop exceeded its iteration bound");
   return ZT_OK;
 }
 
@@ -351,6 +677,7 @@ zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cf
   if (rc == ZT_OK) {
     cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "render / copy framebuffer");
+    else rc = wavefront_status(s, cfg);
   }
   cudaFree(d_out);
   return rc;

@@ -181,7 +181,14 @@ ZT_D bool plane_t(dv3 point, dv3 normal, dv3 o, dv3 d, double tmin, double tmax,
   return true;
 }
 
-ZT_D bool prim_t(const DPrim& p, dv3 o, dv3 d, double tmin, double tmax, double& t) {
+ZT_D bool prim_t(const DPrim& pg, dv3 o, dv3 d, double tmin, double tmax, double& t) {
+  /* five 16-byte read-only loads of the 80-byte record */
+  const double2* q = reinterpret_cast<const double2*>(&pg);
+  const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+  DPrim p;
+  p.a[0] = q0.x; p.a[1] = q0.y; p.a[2] = q1.x; p.a[3] = q1.y; p.a[4] = q2.x;
+  p.a[5] = q2.y; p.a[6] = q3.x; p.a[7] = q3.y; p.a[8] = q4.x;
+  p.kind = (uint32_t)((unsigned long long)__double_as_longlong(q4.y) >> 32); /* material, kind */
   if (p.kind == kTriangle) return triangle_t(L3(p.a), L3(p.a + 3), L3(p.a + 6), o, d, tmin, tmax, t);
   if (p.kind == kSphere) return sphere_t(L3(p.a), p.a[3], o, d, tmin, tmax, t);
   return plane_t(L3(p.a), L3(p.a + 3), o, d, tmin, tmax, t);
@@ -230,58 +237,83 @@ struct StackEntry { uint32_t first, count; double t; };
  * so whether a hit exists is the same answer the reference's closest-hit
  * query gives to `!= null` (render.zig:51). */
 template <bool kAnyHit>
+ZT_D int32_t scene_query(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out);
+
+/* The hit record of a query result (prim code k at distance t). */
+ZT_D void hit_from(const DevScene& sc, int32_t k, dv3 o, dv3 d, double t, Hit& out) {
+  if (k >= 0) {
+    prim_hit(sc.prims[k], o, d, t, out);
+    out.prim = sc.prim_ids[k];
+  } else {
+    const int32_t pi = -2 - k;
+    prim_hit(sc.planes[pi], o, d, t, out);
+    out.prim = (int32_t)sc.n_prims + pi;
+  }
+}
+
+template <bool kAnyHit>
 ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, Hit& out) {
+  double t;
+  const int32_t k = scene_query<kAnyHit>(sc, o, d, tmin, tmax, t);
+  if (k == -1) return false;
+  out.t = t;
+  if (!kAnyHit) hit_from(sc, k, o, d, t, out);
+  return true;
+}
+
+/* Returns the prim code of the closest hit (>= 0: prims[k]; <= -2:
+ * planes[-2 - k]; -1: no hit) and its distance. */
+template <bool kAnyHit>
+ZT_D int32_t scene_query(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out) {
   double closest = tmax;
   int32_t best_k = -1;  /* >= 0: prims[best_k]; <= -2: planes[-2 - best_k] */
-  if (sc.has_root) {
-    const dv3 inv = V(1.0 / d.x, 1.0 / d.y, 1.0 / d.z);
+  double t;
+  const dv3 inv = V(1.0 / d.x, 1.0 / d.y, 1.0 / d.z); /* aabb.zig:86-88 */
+  if (sc.has_root && slab(sc.root_lo, sc.root_hi, o, inv, tmin, closest, t)) {
+    /* Nearest-first stack traversal, bvh.zig:94-124: one pop per step. */
     StackEntry stack[kStackSize];
-    int sp = 0;
-    double t;
-    if (slab(sc.root_lo, sc.root_hi, o, inv, tmin, closest, t)) {
-      stack[0].first = sc.root_first;
-      stack[0].count = sc.root_count;
-      stack[0].t = t;
-      sp = 1;
-    }
+    stack[0].first = sc.root_first;
+    stack[0].count = sc.root_count;
+    stack[0].t = t;
+    int sp = 1;
     while (sp > 0) {
       --sp;
       const StackEntry e = stack[sp];
-      if (e.t > closest) continue;
+      if (e.t > closest) continue; /* bvh.zig:97 */
       if (e.count > 0) {
         for (uint32_t k = e.first; k < e.first + e.count; ++k) {
           double th;
           if (prim_t(sc.prims[k], o, d, tmin, closest, th)) {
             closest = th;
             best_k = (int32_t)k;
-            if (kAnyHit) { out.t = th; return true; }
+            if (kAnyHit) { t_out = th; return best_k; }
           }
         }
         continue;
       }
-      const DPair& pr = sc.pairs[e.first];
+      const double2* rec = reinterpret_cast<const double2*>(sc.pairs + e.first);
+      const double2 a0 = __ldg(rec + 0), a1 = __ldg(rec + 1), a2 = __ldg(rec + 2);
+      const double2 b0 = __ldg(rec + 3), b1 = __ldg(rec + 4), b2 = __ldg(rec + 5);
+      const uint4 pc = __ldg(reinterpret_cast<const uint4*>(rec + 6));
+      /* lo[0] = a0.x a0.y a1.x, lo[1] = a1.y a2.x a2.y, hi[0] = b0.x b0.y b1.x, hi[1] = b1.y b2.x b2.y */
+      const double lo0[3] = {a0.x, a0.y, a1.x}, lo1[3] = {a1.y, a2.x, a2.y};
+      const double hi0[3] = {b0.x, b0.y, b1.x}, hi1[3] = {b1.y, b2.x, b2.y};
       double tl, tr;
-      const bool hl = slab(pr.lo[0], pr.hi[0], o, inv, tmin, closest, tl);
-      const bool hr = slab(pr.lo[1], pr.hi[1], o, inv, tmin, closest, tr);
-      if (hl && hr) {
+      const bool hl = slab(lo0, hi0, o, inv, tmin, closest, tl);
+      const bool hr = slab(lo1, hi1, o, inv, tmin, closest, tr);
+      if (hl && hr) { /* push the farther child first (bvh.zig:111-116) */
         const bool near_left = tl <= tr;
-        const int nf = near_left ? 1 : 0, nn = near_left ? 0 : 1;
-        stack[sp].first = pr.first[nf];
-        stack[sp].count = pr.count[nf];
+        stack[sp].first = near_left ? pc.y : pc.x;
+        stack[sp].count = near_left ? pc.w : pc.z;
         stack[sp].t = near_left ? tr : tl;
-        stack[sp + 1].first = pr.first[nn];
-        stack[sp + 1].count = pr.count[nn];
+        stack[sp + 1].first = near_left ? pc.x : pc.y;
+        stack[sp + 1].count = near_left ? pc.z : pc.w;
         stack[sp + 1].t = near_left ? tl : tr;
         sp += 2;
-      } else if (hl) {
-        stack[sp].first = pr.first[0];
-        stack[sp].count = pr.count[0];
-        stack[sp].t = tl;
-        sp += 1;
-      } else if (hr) {
-        stack[sp].first = pr.first[1];
-        stack[sp].count = pr.count[1];
-        stack[sp].t = tr;
+      } else if (hl || hr) {
+        stack[sp].first = hl ? pc.x : pc.y;
+        stack[sp].count = hl ? pc.z : pc.w;
+        stack[sp].t = hl ? tl : tr;
         sp += 1;
       }
     }
@@ -292,21 +324,11 @@ ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double 
     if (prim_t(sc.planes[i], o, d, tmin, closest, th)) {
       closest = th;
       best_k = -2 - (int32_t)i;
-      if (kAnyHit) { out.t = th; return true; }
+      if (kAnyHit) { t_out = th; return best_k; }
     }
   }
-  if (best_k == -1) return false;
-  if (!kAnyHit) {
-    if (best_k >= 0) {
-      prim_hit(sc.prims[best_k], o, d, closest, out);
-      out.prim = sc.prim_ids[best_k];
-    } else {
-      const int32_t pi = -2 - best_k;
-      prim_hit(sc.planes[pi], o, d, closest, out);
-      out.prim = (int32_t)sc.n_prims + pi;
-    }
-  }
-  return true;
+  t_out = closest;
+  return best_k;
 }
 
 /* ---------------------------------------------------------- Material ---- */

@@ -137,6 +137,24 @@ zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_con
  * must have been uploaded to the current device. */
 zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                            double* d_out_rgb, void* stream);
+/* Allocation-free render, for callers that must not allocate device memory
+ * while rendering: a frame loop recorded into a CUDA graph by stream capture
+ * (a cudaMalloc there breaks the capture), or an engine or service whose own
+ * pool owns the GPU's memory after start-up.  It has no counterpart in the
+ * reference.  The scene must already be resident (zt_scene_upload, which
+ * allocates, belongs at set-up).  The call uses no memory beyond the scene but
+ * a 6 MiB scratch array compiled into the library (held by every GPU that
+ * loads it, for the life of the process): the work counter and a staging
+ * framebuffer of at most ZT_NOALLOC_MAX_PIXELS pixels; larger images are
+ * rejected with ZT_ERR_INVALID_ARGUMENT.  The result is written to the
+ * caller's host buffer (width*height*3 doubles) and the call returns after
+ * synchronising `stream` (a cudaStream_t, NULL = legacy default stream).
+ * The first call on a device looks up the scratch's device address (and may
+ * load the library's GPU code there): make it before any stream capture.
+ * All calls share the scratch, so calls whose GPU work overlaps race. */
+#define ZT_NOALLOC_MAX_PIXELS (512u * 512u)
+#define ZT_NOALLOC_FB_OFFSET 256u
+zt_status zt_render_noalloc(zt_scene* scene, const zt_options* opts, double* out_rgb, void* stream);
 /* First sample of every pixel on the device: primitive id of the camera
  * ray's closest hit (bounded-shape index, or n_bounded + plane index, -1 on a
  * miss) and the number of extension rays the path traced.  Host buffers of

@@ -73,6 +73,7 @@ SIGNATURES = {
     "zt_render_ex": (_i32, [_P, _P, _P, _P]),
     "zt_render_device": (_i32, [_P, _P, _P, _P, _P]),
     "zt_render_debug": (_i32, [_P, _P, _P, _P]),
+    "zt_render_noalloc": (_i32, [_P, _P, _P, _P]),
     "zt_trace_paths": (_i32, [_P, _P, _P, _P, _u64, _u64, _u32, _P]),
     "zt_rng_streams": (_i32, [_u64, _u64, _u64, _u64, _P]),
     "zt_image_to_rgb8": (_i32, [_P, _u64, _u32, C.c_double, C.c_double, _P]),

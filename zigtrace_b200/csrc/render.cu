@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -753,3 +754,103 @@ zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, ui
 }
 
 }  /* extern "C" */
+
+/* ----------------------------------------------- Allocation-free render ---- */
+/*
+ * zt_render_noalloc is for callers that must not allocate device memory once
+ * they are rendering: a frame loop recorded inside CUDA stream capture (a
+ * cudaMalloc there is not a stream operation and breaks the capture), an
+ * engine or service that hands every byte of the GPU to its own pool at
+ * start-up and forbids allocations afterwards, or a real-time loop that cannot
+ * afford the allocator's synchronisation.  The scene is uploaded once at
+ * set-up (zt_scene_upload allocates; do it before the loop).  Per call, the
+ * only device memory used beyond the uploaded scene is the scratch below:
+ * the persistent grid's work counter and a staging framebuffer for at most
+ * ZT_NOALLOC_MAX_PIXELS pixels, copied into the caller's host buffer.
+ *
+ * The array is a file-scope __device__ object: every GPU that loads this
+ * library holds its 6 MiB until the process exits.  All calls share it and it
+ * keeps the last call's contents; the counter is cleared at the start of each
+ * call.  Calls whose GPU work overlaps (different streams or threads at the
+ * same time) race on it.
+ */
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ZT_NOALLOC_FB_OFFSET +
+                                                                 (size_t)ZT_NOALLOC_MAX_PIXELS * 3 * sizeof(double)];
+
+namespace zt {
+
+/* The megakernel writing into the static scratch (counter at offset 0,
+ * framebuffer at ZT_NOALLOC_FB_OFFSET). */
+__global__ void __launch_bounds__(128, 7) k_render_mega_noalloc(DevScene sc, RenderParams p,
+                                                                unsigned char* __restrict__ scratch) {
+  unsigned int* counter = reinterpret_cast<unsigned int*>(scratch);
+  double* out = reinterpret_cast<double*>(scratch + ZT_NOALLOC_FB_OFFSET);
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= tiles) return;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    if (x < p.width && y < p.height) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
+  }
+}
+
+/* In host code g_noalloc_scratch names a host-side stand-in, not device
+ * memory: its device address is looked up once per device, with that device
+ * current, and cached.  The lookup may load this library's GPU code on that
+ * device, which is why the first call on a device belongs before any stream
+ * capture. */
+static std::mutex g_noalloc_mutex;
+static unsigned char* g_noalloc_ptr[256] = {};
+
+static zt_status noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= 256) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return ZT_OK;
+}
+
+}  // namespace zt
+
+extern "C" zt_status zt_render_noalloc(zt_scene* s, const zt_options* o, double* out_rgb, void* stream) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!out_rgb) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_noalloc: NULL output");
+  const uint64_t npix = o->width * o->height;
+  if (npix > ZT_NOALLOC_MAX_PIXELS)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_noalloc: " + std::to_string(o->width) + "x" +
+                                             std::to_string(o->height) + " is " + std::to_string(npix) +
+                                             " pixels, more than its static scratch holds (maximum " +
+                                             std::to_string(ZT_NOALLOC_MAX_PIXELS) + " pixels)");
+  int dev = 0;
+  ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (!s->device || s->device->device != dev)
+    return fail(ZT_ERR_INVALID_ARGUMENT,
+                "zt_render_noalloc: scene is not resident on the current device; call zt_scene_upload at set-up");
+  unsigned char* scratch = nullptr;
+  rc = noalloc_scratch(dev, &scratch);
+  if (rc != ZT_OK) return rc;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const RenderParams p = make_params(s, o);
+  double* fb = reinterpret_cast<double*>(scratch + ZT_NOALLOC_FB_OFFSET);
+  const size_t bytes = (size_t)npix * 3 * sizeof(double);
+  if (p.max_depth == 0) { /* traceWith never enters its loop: every sample is zero */
+    ZT_CUDA(cudaMemsetAsync(fb, 0, bytes, st), "clear framebuffer");
+  } else {
+    ZT_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned int), st), "clear work counter");
+    k_render_mega_noalloc<<<persistent_grid(k_render_mega_noalloc, 128, npix), 128, 0, st>>>(launch_view(s), p,
+                                                                                          scratch);
+    ZT_CUDA(cudaGetLastError(), "launch k_render_mega_noalloc");
+  }
+  ZT_CUDA(cudaMemcpyAsync(out_rgb, fb, bytes, cudaMemcpyDeviceToHost, st), "copy framebuffer");
+  ZT_CUDA(cudaStreamSynchronize(st), "zt_render_noalloc");
+  return ZT_OK;
+}

@@ -236,8 +236,12 @@ struct StackEntry { uint32_t first, count; double t; };
  * at the first primitive hit: the traversal up to that point is identical,
  * so whether a hit exists is the same answer the reference's closest-hit
  * query gives to `!= null` (render.zig:51). */
+ZT_D int32_t scene_query_rt(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, bool any_hit,
+                            double& t_out);
 template <bool kAnyHit>
-ZT_D int32_t scene_query(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out);
+ZT_D int32_t scene_query(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out) {
+  return scene_query_rt(sc, o, d, tmin, tmax, kAnyHit, t_out);
+}
 
 /* The hit record of a query result (prim code k at distance t). */
 ZT_D void hit_from(const DevScene& sc, int32_t k, dv3 o, dv3 d, double t, Hit& out) {
@@ -262,9 +266,10 @@ ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double 
 }
 
 /* Returns the prim code of the closest hit (>= 0: prims[k]; <= -2:
- * planes[-2 - k]; -1: no hit) and its distance. */
-template <bool kAnyHit>
-ZT_D int32_t scene_query(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out) {
+ * planes[-2 - k]; -1: no hit) and its distance.  any_hit is a run-time flag
+ * so that lanes with closest-hit and any-hit queries share one traversal. */
+ZT_D int32_t scene_query_rt(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, bool kAnyHit,
+                            double& t_out) {
   double closest = tmax;
   int32_t best_k = -1;  /* >= 0: prims[best_k]; <= -2: planes[-2 - best_k] */
   double t;

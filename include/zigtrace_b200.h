@@ -95,6 +95,8 @@ zt_status zt_scene_create(zt_scene** out);
 void zt_scene_destroy(zt_scene* scene);
 /* Scene.addMaterial; writes the new material id. */
 zt_status zt_scene_add_material(zt_scene* scene, const zt_material* m, uint32_t* id_out);
+/* Scene.addMaterial for n materials; writes the id of the first one. */
+zt_status zt_scene_add_materials(zt_scene* scene, const zt_material* m, size_t n, uint32_t* first_id_out);
 /* Scene.add for n shapes; planes go to the unbounded list (scene.zig:71-78).
  * Invalidates a previous build. */
 zt_status zt_scene_add_shapes(zt_scene* scene, const zt_shape* shapes, size_t n);
@@ -137,6 +139,24 @@ zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_con
  * must have been uploaded to the current device. */
 zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                            double* d_out_rgb, void* stream);
+/* ---- Batched form: many renders in one persistent launch --------------- */
+/* n renders (scenes[i] with opts[i] into the device buffer d_outs[i] of
+ * width*height*3 doubles) prepared as one persistent kernel launch captured
+ * in a CUDA graph.  Every pixel equals what zt_render gives for that scene
+ * and those options.  order: 0 = tiles in the given order, 1 = largest
+ * renders first.  Scenes are uploaded to the current device if needed.  The
+ * batch keeps pointers to the scenes' device copies: destroy it before the
+ * scenes change or are destroyed.  block_size in cfg: 0/64/128/256. */
+typedef struct zt_batch zt_batch;
+zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint64_t n, double* const* d_outs,
+                          const zt_gpu_config* cfg, uint32_t order, zt_batch** out);
+/* Replays the batch's graph on `stream` (a cudaStream_t) without waiting. */
+zt_status zt_batch_launch(zt_batch* batch, void* stream);
+void zt_batch_destroy(zt_batch* batch);
+/* Convenience: the batch into host buffers outs[i] (blocking). */
+zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint64_t n, double* const* outs,
+                          const zt_gpu_config* cfg);
+
 /* Allocation-free render, for callers that must not allocate device memory
  * while rendering: a frame loop recorded into a CUDA graph by stream capture
  * (a cudaMalloc there breaks the capture), or an engine or service whose own

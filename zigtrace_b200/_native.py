@@ -56,6 +56,7 @@ SIGNATURES = {
     "zt_scene_create": (_i32, [C.POINTER(_P)]),
     "zt_scene_destroy": (None, [_P]),
     "zt_scene_add_material": (_i32, [_P, _P, C.POINTER(_u32)]),
+    "zt_scene_add_materials": (_i32, [_P, _P, C.c_size_t, C.POINTER(_u32)]),
     "zt_scene_add_shapes": (_i32, [_P, _P, C.c_size_t]),
     "zt_scene_add_quad": (_i32, [_P, _P, _P, _P, _u32]),
     "zt_scene_set_camera": (_i32, [_P, _P]),
@@ -74,6 +75,10 @@ SIGNATURES = {
     "zt_render_device": (_i32, [_P, _P, _P, _P, _P]),
     "zt_render_debug": (_i32, [_P, _P, _P, _P]),
     "zt_render_noalloc": (_i32, [_P, _P, _P, _P]),
+    "zt_batch_create": (_i32, [_P, _P, _u64, _P, _P, _u32, C.POINTER(_P)]),
+    "zt_batch_launch": (_i32, [_P, _P]),
+    "zt_batch_destroy": (None, [_P]),
+    "zt_render_batch": (_i32, [_P, _P, _u64, _P, _P]),
     "zt_trace_paths": (_i32, [_P, _P, _P, _P, _u64, _u64, _u32, _P]),
     "zt_rng_streams": (_i32, [_u64, _u64, _u64, _u64, _P]),
     "zt_image_to_rgb8": (_i32, [_P, _u64, _u32, C.c_double, C.c_double, _P]),

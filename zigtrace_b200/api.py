@@ -191,6 +191,13 @@ class Scene:
         self._invalidate()
         return len(self._mats) - 1
 
+    def add_materials(self, mats: np.ndarray) -> int:
+        """Vectorised Scene.addMaterial; returns the id of the first one."""
+        first = len(self._mats)
+        self._mats.extend(np.ascontiguousarray(mats, N.MATERIAL_DTYPE).reshape(-1))
+        self._invalidate()
+        return first
+
     def add(self, shape: np.void) -> None:
         self.add_shapes(np.array([shape], N.SHAPE_DTYPE))
 
@@ -254,8 +261,8 @@ class Scene:
         N.check(lib.zt_scene_create(C.byref(h)))
         self._handle = h
         mats = self.materials
-        for i in range(len(mats)):
-            N.check(lib.zt_scene_add_material(h, N.ptr(mats[i:i + 1]), None))
+        if len(mats):
+            N.check(lib.zt_scene_add_materials(h, N.ptr(mats), len(mats), None))
         shapes = self.shapes
         if len(shapes):
             N.check(lib.zt_scene_add_shapes(h, N.ptr(shapes), len(shapes)))
@@ -379,6 +386,52 @@ def render_device(scene: Scene, opts: Options, d_out_ptr: int, stream_ptr: int,
     cfg = gpu.record() if gpu is not None else None
     N.check(N.lib().zt_render_device(scene.handle, N.ptr(rec), N.ptr(cfg) if cfg is not None else None,
                                      C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr)))
+
+
+class Batch:
+    """A prepared batch of renders (zt_batch): one persistent launch over all
+    images, captured in a CUDA graph and replayed by ``launch``.  Outputs are
+    device buffers given as integer addresses (e.g. ``tensor.data_ptr()``).
+    order 1 puts the largest renders first."""
+
+    def __init__(self, scenes, opts_list, d_out_ptrs, gpu: Optional[GpuConfig] = None, order: int = 1):
+        n = len(scenes)
+        assert n == len(opts_list) == len(d_out_ptrs) and n > 0
+        self._scenes = list(scenes)  # keep the scenes (and their device copies) alive
+        handles = (C.c_void_p * n)(*[s.handle.value for s in scenes])
+        recs = np.concatenate([o.record() for o in opts_list])
+        outs = (C.c_void_p * n)(*[int(p) for p in d_out_ptrs])
+        cfg = gpu.record() if gpu is not None else None
+        h = C.c_void_p()
+        N.check(N.lib().zt_batch_create(handles, N.ptr(recs), n, outs, N.ptr(cfg) if cfg is not None else None,
+                                        order, C.byref(h)))
+        self._h = h
+
+    def launch(self, stream_ptr: int = 0) -> None:
+        N.check(N.lib().zt_batch_launch(self._h, C.c_void_p(stream_ptr)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.lib().zt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render_batch(scenes, opts_list, gpu: Optional[GpuConfig] = None):
+    """Many renders in one persistent launch; returns one Image per render."""
+    n = len(scenes)
+    outs = [np.zeros(int(o.width) * int(o.height) * 3, np.float64) for o in opts_list]
+    handles = (C.c_void_p * n)(*[s.handle.value for s in scenes])
+    recs = np.concatenate([o.record() for o in opts_list])
+    ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+    cfg = gpu.record() if gpu is not None else None
+    N.check(N.lib().zt_render_batch(handles, N.ptr(recs), n, ptrs, N.ptr(cfg) if cfg is not None else None))
+    return [Image(int(o.width), int(o.height), a.reshape(-1, 3)) for o, a in zip(opts_list, outs)]
 
 
 def render_debug(scene: Scene, opts: Options):

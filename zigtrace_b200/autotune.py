@@ -1,0 +1,136 @@
+"""Autotuner for the device execution choices.
+
+For a render it times the megakernel at block sizes 64/128/256 and the
+wavefront form; for a batch it times block sizes 64/128/256 with the renders
+in the given order or largest first.  Every candidate renders identical
+pixels (the choice only changes scheduling), so the fastest one is kept.
+Results are cached per (GPU, scene class) in a JSON file, by default
+``~/.cache/zigtrace_b200/autotune.json`` (override with ZT_AUTOTUNE_CACHE).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import statistics
+from pathlib import Path
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+from .api import MODE_MEGAKERNEL, MODE_WAVEFRONT, Batch, GpuConfig, Options, Scene, render_device
+
+SINGLE_CANDIDATES: List[Tuple[int, int, int]] = [  # (mode, block_size, queue_capacity)
+    (MODE_MEGAKERNEL, 64, 0), (MODE_MEGAKERNEL, 128, 0), (MODE_MEGAKERNEL, 256, 0), (MODE_WAVEFRONT, 128, 0)]
+BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)]
+
+
+def cache_path() -> Path:
+    return Path(os.environ.get("ZT_AUTOTUNE_CACHE", str(Path.home() / ".cache" / "zigtrace_b200" / "autotune.json")))
+
+
+def _load() -> Dict:
+    try:
+        return json.loads(cache_path().read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(key: str, entry: Dict) -> None:
+    data = _load()
+    data[key] = entry
+    p = cache_path()
+    p.parent.mkdir(parents=True, exist_ok=True)
+    tmp = p.with_suffix(".tmp")
+    tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+    tmp.replace(p)
+
+
+def gpu_key() -> str:
+    import torch
+    p = torch.cuda.get_device_properties(torch.cuda.current_device())
+    return f"{p.name}|sm{p.major}{p.minor}|{p.multi_processor_count}SM"
+
+
+def _mag(x: float) -> int:
+    return int(round(math.log10(max(x, 1.0))))
+
+
+def scene_class(scene: Scene, opts: Options) -> str:
+    """Coarse class of a render: orders of magnitude of primitives and
+    pixels, whether it has lights, spp, depth, light sampling."""
+    c = scene.counts()
+    return (f"prims1e{_mag(c['bounded'] + c['planes'])}|lights{int(c['lights'] > 0)}|px1e{_mag(opts.width * opts.height)}"
+            f"|spp{opts.spp}|depth{opts.max_depth}|nee{int(opts.light_sampling)}")
+
+
+def batch_class(scenes: Sequence[Scene], opts: Sequence[Options]) -> str:
+    px = sum(o.width * o.height for o in opts)
+    prims = sum(s.counts()["bounded"] for s in scenes) / len(scenes)
+    return f"batch|n{len(scenes)}|px1e{_mag(px)}|meanprims1e{_mag(prims)}|spp{opts[0].spp}|depth{opts[0].max_depth}"
+
+
+def _event_timer(fn: Callable[[], None], reps: int) -> float:
+    """Median device milliseconds of fn() on the current stream."""
+    import torch
+    stream = torch.cuda.current_stream()
+    fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def choose(key: str, candidates: Sequence, run: Callable, reps: int = 2, use_cache: bool = True,
+           timer: Callable[[Callable[[], None], int], float] = _event_timer):
+    """Returns the fastest candidate for `key`, timing each with run(c) once
+    per rep unless the cache already holds a choice."""
+    if use_cache:
+        hit = _load().get(key)
+        if hit is not None and hit.get("best") is not None:
+            return tuple(hit["best"]), hit["ms"], True
+    ms = {}
+    for c in candidates:
+        ms[json.dumps(list(c))] = timer(lambda: run(c), reps)
+    best = min(ms, key=ms.get)
+    _store(key, {"best": json.loads(best), "ms": ms})
+    return tuple(json.loads(best)), ms, False
+
+
+def tune_render(scene: Scene, opts: Options, reps: int = 2, use_cache: bool = True) -> GpuConfig:
+    """Fastest device configuration for rendering `scene` with `opts`."""
+    import torch
+    scene.upload()
+    out = torch.empty(opts.width * opts.height * 3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def run(c):
+        render_device(scene, opts, out.data_ptr(), stream, GpuConfig(mode=c[0], block_size=c[1], queue_capacity=c[2]))
+
+    best, _, _ = choose(f"{gpu_key()}|render|{scene_class(scene, opts)}", SINGLE_CANDIDATES, run, reps, use_cache)
+    return GpuConfig(mode=best[0], block_size=best[1], queue_capacity=best[2])
+
+
+def tune_batch(scenes: Sequence[Scene], opts: Sequence[Options], reps: int = 2,
+               use_cache: bool = True) -> Tuple[GpuConfig, int, Dict, bool]:
+    """Fastest (block size, order) for a batch; returns (config, order,
+    timings in ms, whether it came from the cache)."""
+    import torch
+    outs = [torch.empty(o.width * o.height * 3, dtype=torch.float64, device="cuda") for o in opts]
+    stream = torch.cuda.current_stream().cuda_stream
+    batches = {}
+
+    def run(c):
+        if c not in batches:
+            batches[c] = Batch(scenes, opts, [t.data_ptr() for t in outs], GpuConfig(block_size=c[0]), order=c[1])
+        batches[c].launch(stream)
+
+    best, ms, cached = choose(f"{gpu_key()}|{batch_class(scenes, opts)}", BATCH_CANDIDATES, run, reps, use_cache)
+    torch.cuda.synchronize()
+    for b in batches.values():
+        b.close()
+    return GpuConfig(block_size=best[0]), best[1], ms, cached

@@ -10,8 +10,10 @@
  * persistent grid that takes pixel batches from a device work counter.
  */
 #include <cuda_runtime.h>
+#include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <new>
 #include <string>
@@ -231,14 +233,14 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
   }
 }
 
-/* Persistent megakernel: each warp takes 32 consecutive pixels from the
- * device work counter until the image is exhausted (the device form of
- * Context.work's atomic tile counter, render.zig:113-119). */
-/* 7 blocks of 128 per SM (<= 73 registers): measured fastest on the
- * 1M-triangle workload among 4..8 blocks per SM. */
-__global__ void __launch_bounds__(128, 7) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
-                                                     unsigned int* __restrict__ counter) {
-  /* A warp renders an 8x4 pixel tile, so its camera rays are coherent. */
+/* Persistent megakernel: each warp takes an 8x4 pixel tile from the device
+ * work counter until the image is exhausted (the device form of
+ * Context.work's atomic tile counter, render.zig:113-119), so its camera rays
+ * are coherent.  896 resident threads per SM (7 blocks of 128, <= 73
+ * registers) measured fastest on the 1M-triangle workload among 512..1024. */
+template <int BS>
+__global__ void __launch_bounds__(BS, 896 / BS) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
+                                                            unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
@@ -248,6 +250,43 @@ __global__ void __launch_bounds__(128, 7) k_render_mega(DevScene sc, RenderParam
     if ((uint64_t)tile >= tiles) return;
     const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
     if (x < p.width && y < p.height) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
+  }
+}
+
+/* One render of a batch: its scene view, parameters, output and the index
+ * of its first tile in the batch-wide tile numbering. */
+struct BatchItem {
+  DevScene sc;
+  RenderParams p;
+  double* out;
+  uint64_t tile_begin;
+  uint64_t tiles_x;
+};
+
+/* Batched persistent launch: many renders of uneven size share one grid.
+ * Warps take 8x4 tiles from one counter over the concatenated tile ranges of
+ * all items (in the order the host chose, largest first by default) and
+ * render them with the item's own scene and parameters, so small images do
+ * not leave the GPU idle the way one launch per image does. */
+template <int BS>
+__global__ void __launch_bounds__(BS, 896 / BS) k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items,
+                                                             uint64_t total_tiles, unsigned int* __restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= total_tiles) return;
+    uint32_t lo = 0, hi = n_items - 1; /* last item with tile_begin <= tile */
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) / 2;
+      if (items[mid].tile_begin <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchItem& it = items[lo];
+    const uint64_t local = tile - it.tile_begin;
+    const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
+    if (x < it.p.width && y < it.p.height) render_pixel<false>(it.sc, it.p, y * it.p.width + x, it.out, nullptr);
   }
 }
 
@@ -476,11 +515,23 @@ static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
   return (unsigned)(blocks > 0 ? blocks : 1);
 }
 
-static zt_status launch_mega(zt_scene* s, const RenderParams& p, double* d_out, cudaStream_t stream) {
+template <int BS>
+static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
+                           cudaStream_t stream) {
+  k_render_mega<BS><<<persistent_grid(k_render_mega<BS>, BS, p.width * p.height), BS, 0, stream>>>(v, p, d_out,
+                                                                                                  counter);
+}
+
+static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
+
+static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out,
+                             cudaStream_t stream) {
   zt_device_buffers* d = s->device;
   ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
-  const unsigned blocks = persistent_grid(k_render_mega, 128, p.width * p.height);
-  k_render_mega<<<blocks, 128, 0, stream>>>(launch_view(s), p, d_out, d->counter);
+  const DevScene v = launch_view(s);
+  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, stream);
+  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, stream);
+  else launch_mega_bs<128>(v, p, d_out, d->counter, stream);
   ZT_CUDA(cudaGetLastError(), "launch k_render_mega");
   return ZT_OK;
 }
@@ -609,7 +660,9 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   const uint32_t mode = cfg ? cfg->mode : ZT_MODE_AUTO;
   if (mode == ZT_MODE_WAVEFRONT) return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
   if (mode > ZT_MODE_WAVEFRONT) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
-  return launch_mega(s, p, d_out, stream);
+  const uint32_t bs = cfg ? cfg->block_size : 0;
+  if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
+  return launch_mega(s, p, bs, d_out, stream);
 }
 
 /* Error word of the last wavefront launch (after the stream is idle). */
@@ -751,6 +804,146 @@ zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, ui
   cudaFree(d);
   if (e != cudaSuccess) return cuda_fail(e, "rng streams");
   return ZT_OK;
+}
+
+}  /* extern "C" */
+
+/* --------------------------------------------------------- Batched form ---- */
+/* A prepared batch: the items table on the device and an executable graph
+ * holding [reset counter, one persistent k_render_batch launch]. */
+struct zt_batch {
+  int device = -1;
+  uint64_t n = 0;
+  uint64_t total_tiles = 0;
+  uint32_t block_size = 128;
+  BatchItem* d_items = nullptr;
+  unsigned int* d_counter = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace zt {
+
+template <int BS>
+static void launch_batch_bs(const zt_batch* b, cudaStream_t st) {
+  k_render_batch<BS><<<persistent_grid(k_render_batch<BS>, BS, b->total_tiles * 32), BS, 0, st>>>(
+      b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
+}
+
+static void batch_free(zt_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  cudaFree(b->d_items);
+  cudaFree(b->d_counter);
+  delete b;
+}
+
+}  // namespace zt
+
+extern "C" {
+
+zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint64_t n, double* const* d_outs,
+                          const zt_gpu_config* cfg, uint32_t order, zt_batch** out) {
+  if (!scenes || !opts || !d_outs || !out || n == 0 || n > 0xFFFFFFFFull)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: NULL argument or empty batch");
+  *out = nullptr;
+  const uint32_t bs = cfg ? cfg->block_size : 0;
+  if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
+  if (order > 1) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: order must be 0 (as given) or 1 (largest first)");
+  std::vector<uint64_t> idx(n);
+  std::vector<double> cost(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    zt_status rc = check_render_args(scenes[i], &opts[i]);
+    if (rc != ZT_OK) return rc;
+    if (!d_outs[i]) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: NULL output");
+    rc = upload(scenes[i]);
+    if (rc != ZT_OK) return rc;
+    idx[i] = i;
+    /* expected work: samples x log2 of the primitive count */
+    cost[i] = (double)(opts[i].width * opts[i].height * opts[i].spp) *
+              log2((double)scenes[i]->shapes.size() + scenes[i]->planes.size() + 2.0);
+  }
+  if (order == 1) std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return cost[a] > cost[b]; });
+  std::vector<BatchItem> items(n);
+  uint64_t tiles = 0;
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint64_t i = idx[k];
+    BatchItem& it = items[k];
+    it.sc = launch_view(scenes[i]);
+    it.p = make_params(scenes[i], &opts[i]);
+    it.out = d_outs[i];
+    it.tiles_x = (opts[i].width + 7) / 8;
+    it.tile_begin = tiles;
+    tiles += it.tiles_x * ((opts[i].height + 3) / 4);
+  }
+  if (tiles >= (1ull << 32)) return fail(ZT_ERR_INVALID_OPTIONS, "zt_batch_create: more than 2^32 tiles in the batch");
+  for (uint64_t k = 0; k < n; ++k)
+    if (items[k].p.max_depth == 0)
+      return fail(ZT_ERR_INVALID_OPTIONS, "zt_batch_create: max_depth 0 renders are all zero; render them alone");
+  zt_batch* b = new (std::nothrow) zt_batch();
+  if (!b) return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory");
+  b->n = n;
+  b->total_tiles = tiles;
+  b->block_size = bs ? bs : 128;
+  cudaError_t e = cudaGetDevice(&b->device);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_items, n * sizeof(BatchItem));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_items, items.data(), n * sizeof(BatchItem), cudaMemcpyHostToDevice);
+  cudaStream_t cs = nullptr;
+  cudaGraph_t g = nullptr;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned int), cs);
+    if (b->block_size == 64) launch_batch_bs<64>(b, cs);
+    else if (b->block_size == 256) launch_batch_bs<256>(b, cs);
+    else launch_batch_bs<128>(b, cs);
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    e = e2 != cudaSuccess ? e2 : cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (cs) cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    batch_free(b);
+    return cuda_fail(e, "zt_batch_create");
+  }
+  *out = b;
+  return ZT_OK;
+}
+
+zt_status zt_batch_launch(zt_batch* b, void* stream) {
+  if (!b) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_launch: NULL batch");
+  ZT_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream), "zt_batch_launch");
+  return ZT_OK;
+}
+
+void zt_batch_destroy(zt_batch* b) { batch_free(b); }
+
+zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint64_t n, double* const* outs,
+                          const zt_gpu_config* cfg) {
+  if (!scenes || !opts || !outs || n == 0) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_batch: NULL argument");
+  std::vector<size_t> off(n + 1, 0);
+  for (uint64_t i = 0; i < n; ++i) {
+    if (!opts[i].width || !opts[i].height) return fail(ZT_ERR_INVALID_OPTIONS, "InvalidOptions");
+    off[i + 1] = off[i] + (size_t)(opts[i].width * opts[i].height * 3);
+  }
+  double* d = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d, off[n] * sizeof(double)), "allocate batch framebuffers");
+  std::vector<double*> d_outs(n);
+  for (uint64_t i = 0; i < n; ++i) d_outs[i] = d + off[i];
+  zt_batch* b = nullptr;
+  zt_status rc = zt_batch_create(scenes, opts, n, d_outs.data(), cfg, 1, &b);
+  if (rc == ZT_OK) rc = zt_batch_launch(b, nullptr);
+  if (rc == ZT_OK) {
+    for (uint64_t i = 0; i < n && rc == ZT_OK; ++i) {
+      const cudaError_t e = cudaMemcpy(outs[i], d_outs[i], (off[i + 1] - off[i]) * sizeof(double),
+                                       cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = cuda_fail(e, "copy batch framebuffer");
+    }
+  }
+  zt_batch_destroy(b);
+  cudaFree(d);
+  return rc;
 }
 
 }  /* extern "C" */

@@ -457,6 +457,22 @@ zt_status zt_scene_add_material(zt_scene* s, const zt_material* m, uint32_t* id_
   return ZT_OK;
 }
 
+zt_status zt_scene_add_materials(zt_scene* s, const zt_material* m, size_t n, uint32_t* first_id_out) {
+  if (!s || (!m && n)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_add_materials: NULL argument");
+  for (size_t i = 0; i < n; ++i)
+    if (m[i].kind > ZT_EMISSIVE) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown material kind");
+  if (s->materials.size() + n > 0xFFFFFFFFull) return fail(ZT_ERR_INVALID_ARGUMENT, "too many materials");
+  release_staging(s);
+  s->built = false;
+  if (first_id_out) *first_id_out = (uint32_t)s->materials.size();
+  try {
+    s->materials.insert(s->materials.end(), m, m + n);
+  } catch (const std::bad_alloc&) {
+    return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory");
+  }
+  return ZT_OK;
+}
+
 zt_status zt_scene_add_shapes(zt_scene* s, const zt_shape* shapes, size_t n) { /* Scene.add */
   if (!s || (!shapes && n)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_add_shapes: NULL argument");
   for (size_t i = 0; i < n; ++i)

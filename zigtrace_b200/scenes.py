@@ -202,6 +202,58 @@ def triangle_heavy(seed: int = 0, nx: int = 1000, nz: int = 500, n_ico: int = 20
 
 TRIANGLE_HEAVY_OPTIONS = Options(width=1920, height=1080, spp=64, max_depth=16, seed=0)
 
+
+# --------------------------------------------------------- batched form ----
+def sphere_field(seed: int, n: int) -> Scene:
+    """Ground plane + exactly n r=0.2 spheres on a jittered grid sized to n
+    (spacing as in random_spheres), 80/15/5 Lambertian/metal/glass, sky
+    background, thin-lens camera framing the field."""
+    from .api import LAMBERTIAN, METAL, DIELECTRIC
+    from . import _native as N
+    rng = np.random.default_rng(seed)
+    g = int(math.ceil(math.sqrt(n)))
+    cell = 22.0 / 18.0
+    extent = g * cell / 2.0
+    cells = rng.permutation(g * g)[:n]
+    i, j = cells // g, cells % g
+    cx = -extent + (i + 0.05 + 0.9 * rng.random(n)) * cell
+    cz = -extent + (j + 0.05 + 0.9 * rng.random(n)) * cell
+    choose = rng.random(n)
+    s = Scene()
+    s.background = Background.sky((1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
+    ground = s.add_material(Material.lambertian((0.5, 0.5, 0.5)))
+    s.add(plane((0.0, 0.0, 0.0), (0.0, 1.0, 0.0), ground))
+    mats = np.zeros(n, N.MATERIAL_DTYPE)
+    lam, met = choose < 0.8, (choose >= 0.8) & (choose < 0.95)
+    gl = ~(lam | met)
+    mats["kind"] = np.where(lam, LAMBERTIAN, np.where(met, METAL, DIELECTRIC))
+    mats["color"][lam] = rng.random((int(lam.sum()), 3)) * rng.random((int(lam.sum()), 3))
+    mats["color"][met] = rng.uniform(0.5, 1.0, (int(met.sum()), 3))
+    mats["param"][met] = rng.uniform(0.0, 0.5, int(met.sum()))
+    mats["param"][gl] = 1.5
+    first = s.add_materials(mats)
+    s.add_spheres(np.stack([cx, np.full(n, 0.2), cz], axis=1), np.full(n, 0.2), first + np.arange(n))
+    k = max(extent / 11.0, 0.25)
+    s.camera = CameraConfig(look_from=(13 * k, 2 * k, 3 * k), look_at=(0, 0, 0), vfov=20, aperture=0.1 * k,
+                            focus_dist=10.0 * k)
+    return s
+
+
+BATCH_RESOLUTIONS = ((64, 64), (128, 128), (256, 256), (512, 288))
+
+
+def batch_workload(count: int = 256, seed: int = 0, spp: int = 16, max_depth: int = 16):
+    """The batched form's renders: scene k is a sphere field from its own
+    seed with a sphere count log-uniform in [16, 20000] and a resolution drawn
+    from BATCH_RESOLUTIONS; returns [(scene, Options)]."""
+    rng = np.random.default_rng(seed + 77)
+    out = []
+    for k in range(count):
+        n = int(math.floor(math.exp(rng.uniform(math.log(16), math.log(20000)))))
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(len(BATCH_RESOLUTIONS)))]
+        out.append((sphere_field(seed + k, n), Options(width=w, height=h, spp=spp, max_depth=max_depth, seed=0)))
+    return out
+
 WORKLOADS = {
     "cornell": (cornell, CORNELL_OPTIONS),
     "random_spheres": (random_spheres, SPHERES_OPTIONS),

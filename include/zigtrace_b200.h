@@ -139,6 +139,22 @@ zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_con
  * must have been uploaded to the current device. */
 zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                            double* d_out_rgb, void* stream);
+/* ---- Differentiable form ------------------------------------------------ */
+/* Gradients of an image loss with respect to every material's colour (the
+ * albedo of Lambertian and metal materials, the radiance of emissive ones;
+ * colors[3*m + c]).  Sampling is detached: the scene's own materials drive
+ * every sampling decision (roulette, light pick, MIS weights), `colors` (NULL
+ * = the scene's own) only the contributions, so with common random numbers
+ * the image is a smooth function of `colors`; with colors == NULL it is
+ * zt_render's image.  zt_forward renders into out_rgb (width*height*3);
+ * zt_backward takes dL/dimage (width*height*3) and writes dL/dcolors
+ * (n_materials*3), replaying each path from its RNG stream (no tape).
+ * Gradients are accumulated with atomics, so their last bits may vary
+ * between runs. */
+zt_status zt_forward(zt_scene* scene, const zt_options* opts, const double* colors, double* out_rgb);
+zt_status zt_backward(zt_scene* scene, const zt_options* opts, const double* colors, const double* d_image,
+                      double* d_colors);
+
 /* ---- Batched form: many renders in one persistent launch --------------- */
 /* n renders (scenes[i] with opts[i] into the device buffer d_outs[i] of
  * width*height*3 doubles) prepared as one persistent kernel launch captured

@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
         _lib.ozt_scene_lights.argtypes = [C.c_void_p] * 4
         _lib.ozt_render.argtypes = [C.c_void_p] * 4
         _lib.ozt_render_debug.argtypes = [C.c_void_p] * 4
+        _lib.ozt_render_params.argtypes = [C.c_void_p] * 4
         _lib.ozt_lights_sample.argtypes = [C.c_void_p] * 7
         _lib.ozt_lights_pdf_hit.argtypes = [C.c_void_p] * 3
         _lib.ozt_material_emitted.argtypes = [C.c_void_p] * 3
@@ -246,6 +247,14 @@ class OracleScene:
             raise ValueError("InvalidOptions")
         if stats:
             return out.reshape(-1, 3), dict(zip(STATS_FIELDS, list(st)))
+        return out.reshape(-1, 3)
+
+    def render_params(self, width, height, spp, max_depth, theta, seed=0, light_sampling=True):
+        """Detached-sampling forward of the differentiable form (theta: n_materials x 3)."""
+        o = self.options(width, height, spp, max_depth, 1, seed, 16, light_sampling)
+        th = np.ascontiguousarray(np.asarray(theta, np.float64).reshape(-1))
+        out = np.zeros(width * height * 3)
+        lib().ozt_render_params(self.h, _p(o), _p(th), _p(out))
         return out.reshape(-1, 3)
 
     def render_debug(self, width, height, max_depth, seed=0, light_sampling=True):

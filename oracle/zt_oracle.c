@@ -869,6 +869,92 @@ static ov3 trace_with(const oscene* s, ov3 ro, ov3 rd, orng* rng, uint64_t max_d
   return radiance;
 }
 
+static int options_valid(const ooptions* o);
+
+/* traceWith with detached sampling for the differentiable form: the scene's
+ * materials drive roulette (throughput tp0), the light pick and the MIS
+ * weights; `theta` (3 per material) drives the contributions.  With theta =
+ * the scene's colours this is trace_with operation for operation. */
+static ov3 trace_params(const oscene* s, const double* theta, ov3 ro, ov3 rd, orng* rng, uint64_t max_depth,
+                        int light_sampling) {
+  const int use_nee = light_sampling && s->n_lights > 0;
+  ov3 radiance = V(0, 0, 0), tp = V(1, 1, 1), tp0 = V(1, 1, 1), prev_origin = V(0, 0, 0);
+  double prev_pdf = 0;
+  for (uint64_t depth = 0; depth < max_depth; ++depth) {
+    ohit hit;
+    if (!scene_intersect(s, ro, rd, RAY_EPSILON, INFINITY, &hit, NULL))
+      return vadd(radiance, vmul(tp, background_radiance(&s->background, rd)));
+    const uint32_t m = hit.material;
+    const omaterial* mat = &s->mats[m];
+    const ov3 th = P3(theta + 3 * (size_t)m);
+    const ov3 le0 = material_emitted(mat, &hit);
+    if (vmaxc(le0) > 0) {
+      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(s, prev_origin, &hit, NULL)) : 1.0;
+      radiance = vadd(radiance, vscale(vmul(tp, th), w));
+    }
+    if (mat->kind == O_LAMBERTIAN && use_nee) {
+      ov3 direct = V(0, 0, 0), ldir, lrad0;
+      double ldist, lpdf;
+      orng probe = *rng;
+      /* which light the pick chooses: light.zig:106-115 on a copy of the stream */
+      const olight* picked = s->n_lights ? lights_pick(s, &probe) : NULL;
+      if (lights_sample(s, hit.point, rng, &ldir, &ldist, &lrad0, &lpdf)) {
+        const double cos_s = vdot(hit.normal, ldir);
+        ohit sh;
+        if (!(cos_s <= 0 || !(lpdf > 0)) &&
+            !scene_intersect(s, hit.point, ldir, RAY_EPSILON, ldist * (1 - 1e-6), &sh, NULL)) {
+          const double bsdf_pdf = cos_s / PI;
+          const double scale = cos_s / (PI * lpdf) * power_weight(lpdf, bsdf_pdf);
+          direct = vscale(vmul(th, P3(theta + 3 * (size_t)picked->shape.material)), scale);
+        }
+      }
+      radiance = vadd(radiance, vmul(tp, direct));
+    }
+    ov3 atten0, so, sd;
+    if (!material_scatter(mat, rd, &hit, rng, &atten0, &so, &sd)) break;
+    const ov3 atten = (mat->kind == O_LAMBERTIAN || mat->kind == O_METAL) ? th : atten0;
+    tp = vmul(tp, atten);
+    tp0 = vmul(tp0, atten0);
+    prev_pdf = (use_nee && mat->kind == O_LAMBERTIAN) ? fmax(vdot(sd, hit.normal), 0) / PI : 0;
+    prev_origin = hit.point;
+    ro = so;
+    rd = sd;
+    if (depth + 1 >= ROULETTE_DEPTH) {
+      const double p = fmin(vmaxc(tp0), 0.95);
+      if (p <= 0 || rng_float(rng) >= p) break;
+      tp = vdiv(tp, p);
+      tp0 = vdiv(tp0, p);
+    }
+  }
+  return radiance;
+}
+
+int ozt_render_params(const oscene* s, const ooptions* o, const double* theta, double* out) {
+  if (!options_valid(o)) return -1;
+  ocamera cam;
+  camera_init(&s->camera, (double)o->width / (double)o->height, &cam);
+  const double w = (double)o->width, h = (double)o->height, inv_spp = 1.0 / (double)o->spp;
+  for (uint64_t y = 0; y < o->height; ++y)
+    for (uint64_t x = 0; x < o->width; ++x) {
+      orng rng = rng_for_stream(o->seed, y * o->width + x);
+      ov3 sum = V(0, 0, 0);
+      for (uint64_t i = 0; i < o->spp; ++i) {
+        const double sx = ((double)x + rng_float(&rng)) / w;
+        const double ty = ((double)y + rng_float(&rng)) / h;
+        ov3 ro, rd;
+        camera_ray(&cam, sx, ty, &rng, &ro, &rd);
+        const ov3 c = trace_params(s, theta, ro, rd, &rng, o->max_depth, (int)o->light_sampling);
+        if (visfinite(c)) sum = vadd(sum, c);
+      }
+      const ov3 px = vscale(sum, inv_spp);
+      double* dst = out + 3 * (y * o->width + x);
+      dst[0] = px.x;
+      dst[1] = px.y;
+      dst[2] = px.z;
+    }
+  return 0;
+}
+
 /* ---------------------------------------------------------------- Render --- */
 /* render.zig:104-180 */
 typedef struct {

@@ -98,6 +98,12 @@ int ozt_render_pixels(const oscene* s, const ooptions* o, const uint64_t* pixels
  * (-1 on a miss) and the number of extension rays the path traced. */
 int ozt_render_debug(const oscene* s, const ooptions* o, int32_t* first_prim, uint32_t* path_len);
 
+/* The differentiable form's forward (detached sampling): the scene's
+ * materials drive roulette, light pick and MIS weights, theta (3 per
+ * material) the contributions.  theta = the scene's colours gives ozt_render's
+ * image.  Single-threaded. */
+int ozt_render_params(const oscene* s, const ooptions* o, const double* theta, double* out_rgb);
+
 /* traceWith (src/render.zig:61-102) on one ray with an explicit RNG state. */
 void ozt_trace_with(const oscene* s, const ov3* origin, const ov3* dir, uint64_t rng[4],
                     uint64_t max_depth, int light_sampling, ov3* out);

@@ -392,6 +392,19 @@ def test_depth_of_field_rays_converge_on_focus_plane():  # camera.zig:90-108
     assert spread > 0
 
 
+# -------------------------------------------------- differentiable form ----
+def test_detached_forward_is_the_render_at_own_colors_and_linear_in_emission():
+    from zigtrace_b200 import scenes
+    scene, target = scenes.cornell_diff()
+    os_ = O.OracleScene.from_scene(scene)
+    theta = np.array([m["color"] for m in scene.materials])
+    base = os_.render_params(20, 20, 2, 8, theta)
+    assert base.tobytes() == os_.render(20, 20, 2, 8, threads=2).tobytes()
+    doubled = theta.copy()
+    doubled[32:] *= 2.0  # every term carries exactly one emitter radiance
+    assert np.allclose(os_.render_params(20, 20, 2, 8, doubled), 2 * base, rtol=1e-12, atol=1e-15)
+
+
 # ---------------------------------------------------------------- image ----
 def test_tone_mapping_curves():  # image.zig:85-101
     assert O.tonemap(1, 1.0) == 0.5 and O.tonemap(0, -3.0) == 0

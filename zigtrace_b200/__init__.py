@@ -12,6 +12,7 @@ radiance path, behind a mirror of the reference library API.
 from .api import (  # noqa: F401
     DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, PLANE, SPHERE, TRIANGLE,
     Background, Batch, CameraConfig, GpuConfig, Image, Material, Options, Output, Scene, Settings, ZigtraceError,
-    plane, render, render_batch, render_debug, render_device, rng_streams, sphere, triangle, write_ppm)
+    backward, forward, plane, render, render_batch, render_debug, render_device, render_function, rng_streams,
+    set_colors, sphere, triangle, write_ppm)
 
 __version__ = "0.1.0"

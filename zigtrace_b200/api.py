@@ -434,6 +434,71 @@ def render_batch(scenes, opts_list, gpu: Optional[GpuConfig] = None):
     return [Image(int(o.width), int(o.height), a.reshape(-1, 3)) for o, a in zip(opts_list, outs)]
 
 
+# ------------------------------------------------------ differentiable form --
+def _colors_arg(scene: Scene, colors):
+    if colors is None:
+        return None
+    c = np.ascontiguousarray(np.asarray(colors, np.float64).reshape(-1))
+    if c.size != 3 * len(scene.materials):
+        raise ZigtraceError(-5, f"colors must hold 3 values per material ({3 * len(scene.materials)})")
+    return c
+
+
+def forward(scene: Scene, opts: Options, colors=None) -> Image:
+    """Image at material colours `colors` (n_materials x 3) with the scene's
+    own colours driving sampling (zt_forward); colors=None gives render()."""
+    c = _colors_arg(scene, colors)
+    out = np.zeros(int(opts.width) * int(opts.height) * 3, np.float64)
+    N.check(N.lib().zt_forward(scene.handle, N.ptr(opts.record()), N.ptr(c) if c is not None else None, N.ptr(out)))
+    return Image(int(opts.width), int(opts.height), out.reshape(-1, 3))
+
+
+def backward(scene: Scene, opts: Options, d_image, colors=None) -> np.ndarray:
+    """dL/dcolors (n_materials x 3) for dL/dimage (width*height x 3), by path
+    replay (zt_backward)."""
+    c = _colors_arg(scene, colors)
+    g = np.ascontiguousarray(np.asarray(d_image, np.float64).reshape(-1))
+    if g.size != int(opts.width) * int(opts.height) * 3:
+        raise ZigtraceError(-5, "d_image must hold width*height*3 values")
+    out = np.zeros(3 * len(scene.materials), np.float64)
+    N.check(N.lib().zt_backward(scene.handle, N.ptr(opts.record()), N.ptr(c) if c is not None else None, N.ptr(g),
+                                N.ptr(out)))
+    return out.reshape(-1, 3)
+
+
+def set_colors(scene: Scene, colors) -> Scene:
+    """Makes `colors` the scene's own material colours (they then also drive
+    sampling) and rebuilds it."""
+    c = np.asarray(colors, np.float64).reshape(-1, 3)
+    mats = scene.materials.copy()
+    mats["color"] = c
+    scene._mats = list(mats)
+    return scene.build()
+
+
+def render_function():
+    """torch.autograd.Function computing the image from material colours:
+    ``img = render_function().apply(colors, scene, opts)`` with colors a
+    float64 tensor (n_materials x 3); backward by path replay."""
+    import torch
+
+    class RenderFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, colors, scene, opts):
+            ctx.scene, ctx.opts = scene, opts
+            c = colors.detach().cpu().numpy()
+            ctx.save_for_backward(colors)
+            return torch.from_numpy(forward(scene, opts, c).pixels.copy()).to(colors.device)
+
+        @staticmethod
+        def backward(ctx, grad_image):
+            (colors,) = ctx.saved_tensors
+            g = backward(ctx.scene, ctx.opts, grad_image.detach().cpu().numpy(), colors.detach().cpu().numpy())
+            return torch.from_numpy(g).to(colors.device), None, None
+
+    return RenderFunction
+
+
 def render_debug(scene: Scene, opts: Options):
     """First-sample primitive ids and path lengths per pixel (device)."""
     n = int(opts.width) * int(opts.height)

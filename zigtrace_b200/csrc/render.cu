@@ -22,6 +22,7 @@
 #include "scene_host.h"
 #include "wavefront.cuh"
 #include "zt_device.cuh"
+#include "zt_diff.cuh"
 
 using namespace zt;
 
@@ -803,6 +804,177 @@ zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, ui
   if (e == cudaSuccess) e = cudaMemcpy(out, d, bytes, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess) return cuda_fail(e, "rng streams");
+  return ZT_OK;
+}
+
+}  /* extern "C" */
+
+/* --------------------------------------------------- Differentiable form ---- */
+namespace zt {
+
+/* Forward of the detached estimator (zt_diff.cuh): the megakernel's tile
+ * loop with trace_diff; theta == the scene's colours gives zt_render's image. */
+template <int BS>
+__global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, RenderParams p,
+                                                             const double* __restrict__ theta,
+                                                             double* __restrict__ out, unsigned int* __restrict__ counter) {
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= tiles) return;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    if (x >= p.width || y >= p.height) continue;
+    const uint64_t pix = y * p.width + x;
+    Rng rng = rng_for_stream(p.seed, pix);
+    dv3 sum = V(0, 0, 0);
+    for (uint64_t i = 0; i < p.spp; ++i) {
+      const double s = ((double)x + rng_float(rng)) / (double)p.width;
+      const double t = ((double)y + rng_float(rng)) / (double)p.height;
+      dv3 ro, rd;
+      camera_ray(p.cam, s, t, rng, ro, rd);
+      const dv3 c = trace_diff<false>(sc, theta, ro, rd, rng, p.max_depth, p.use_nee != 0, V(0, 0, 0), V(0, 0, 0),
+                                      nullptr);
+      if (visfinite(c)) sum = sum + c;
+    }
+    const dv3 px = vscale(sum, 1.0 / (double)p.spp);
+    out[3 * pix + 0] = px.x;
+    out[3 * pix + 1] = px.y;
+    out[3 * pix + 2] = px.z;
+  }
+}
+
+/* Path-replay adjoint: for every sample, the primal pass gives its radiance
+ * L, then the same path is replayed from the saved RNG state accumulating
+ * dL/dtheta into per-block shared memory (flushed once per block), or
+ * straight into global memory when the parameter table is large. */
+template <int BS>
+__global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, RenderParams p,
+                                                              const double* __restrict__ theta,
+                                                              const double* __restrict__ dimg, double* grad,
+                                                              uint32_t n_params, int use_smem,
+                                                              unsigned int* __restrict__ counter) {
+  extern __shared__ double sgrad[];
+  double* g = use_smem ? sgrad : grad;
+  if (use_smem) {
+    for (uint32_t i = threadIdx.x; i < n_params; i += BS) sgrad[i] = 0.0;
+    __syncthreads();
+  }
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const unsigned lane = threadIdx.x & 31;
+  const double inv_spp = 1.0 / (double)p.spp;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= tiles) break;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
+    if (x >= p.width || y >= p.height) continue;
+    const uint64_t pix = y * p.width + x;
+    const dv3 adj = vscale(L3(dimg + 3 * pix), inv_spp); /* pixel = sum * (1/spp), render.zig:144 */
+    if (adj.x == 0 && adj.y == 0 && adj.z == 0) continue;
+    Rng rng = rng_for_stream(p.seed, pix);
+    for (uint64_t i = 0; i < p.spp; ++i) {
+      const double s = ((double)x + rng_float(rng)) / (double)p.width;
+      const double t = ((double)y + rng_float(rng)) / (double)p.height;
+      dv3 ro, rd;
+      camera_ray(p.cam, s, t, rng, ro, rd);
+      Rng replay = rng;
+      const dv3 L = trace_diff<false>(sc, theta, ro, rd, rng, p.max_depth, p.use_nee != 0, V(0, 0, 0), V(0, 0, 0),
+                                      nullptr);
+      if (visfinite(L)) trace_diff<true>(sc, theta, ro, rd, replay, p.max_depth, p.use_nee != 0, L, adj, g);
+    }
+  }
+  if (use_smem) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n_params; i += BS)
+      if (sgrad[i] != 0.0) atomicAdd(grad + i, sgrad[i]);
+  }
+}
+
+/* theta on the device: the caller's colours, or the scene's own. */
+static zt_status upload_theta(const zt_scene* s, const double* colors, double** d_theta) {
+  const size_t n = s->materials.size() * 3;
+  std::vector<double> th(n > 0 ? n : 3, 0.0);
+  for (size_t m = 0; m < s->materials.size(); ++m) {
+    const zt_vec3& c = s->materials[m].color;
+    th[3 * m + 0] = colors ? colors[3 * m + 0] : c.x;
+    th[3 * m + 1] = colors ? colors[3 * m + 1] : c.y;
+    th[3 * m + 2] = colors ? colors[3 * m + 2] : c.z;
+  }
+  ZT_CUDA(cudaMalloc((void**)d_theta, th.size() * sizeof(double)), "allocate parameters");
+  ZT_CUDA(cudaMemcpy(*d_theta, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice), "upload parameters");
+  return ZT_OK;
+}
+
+}  // namespace zt
+
+extern "C" {
+
+zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, double* out) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_forward: NULL output");
+  if ((rc = upload(s)) != ZT_OK) return rc;
+  const RenderParams p = make_params(s, o);
+  const size_t bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  if (p.max_depth == 0) {
+    memset(out, 0, bytes);
+    return ZT_OK;
+  }
+  double *d_theta = nullptr, *d_out = nullptr;
+  if ((rc = upload_theta(s, colors, &d_theta)) != ZT_OK) return rc;
+  cudaError_t e = cudaMalloc((void**)&d_out, bytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
+  if (e == cudaSuccess) {
+    k_forward_diff<128><<<persistent_grid(k_forward_diff<128>, 128, p.width * p.height), 128>>>(
+        launch_view(s), p, d_theta, d_out, s->device->counter);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d_theta);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return cuda_fail(e, "zt_forward");
+  return ZT_OK;
+}
+
+zt_status zt_backward(zt_scene* s, const zt_options* o, const double* colors, const double* d_image,
+                      double* d_colors) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!d_image || !d_colors) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_backward: NULL argument");
+  if ((rc = upload(s)) != ZT_OK) return rc;
+  const RenderParams p = make_params(s, o);
+  const uint32_t n_params = (uint32_t)(s->materials.size() * 3);
+  memset(d_colors, 0, n_params * sizeof(double));
+  if (p.max_depth == 0 || n_params == 0) return ZT_OK;
+  const size_t img_bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  double *d_theta = nullptr, *d_img = nullptr, *d_grad = nullptr;
+  if ((rc = upload_theta(s, colors, &d_theta)) != ZT_OK) return rc;
+  cudaError_t e = cudaMalloc((void**)&d_img, img_bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_grad, n_params * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_img, d_image, img_bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(d_grad, 0, n_params * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
+  if (e == cudaSuccess) {
+    const size_t smem = (size_t)n_params * sizeof(double);
+    const int use_smem = smem <= 32 * 1024 ? 1 : 0;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backward_diff<128>, 128, use_smem ? smem : 0);
+    uint64_t blocks = (uint64_t)sm_count() * (per_sm > 0 ? per_sm : 1);
+    const uint64_t need = (p.width * p.height + 127) / 128;
+    if (blocks > need) blocks = need;
+    k_backward_diff<128><<<(unsigned)blocks, 128, use_smem ? smem : 0>>>(launch_view(s), p, d_theta, d_img, d_grad,
+                                                                         n_params, use_smem, s->device->counter);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(d_colors, d_grad, n_params * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d_theta);
+  cudaFree(d_img);
+  cudaFree(d_grad);
+  if (e != cudaSuccess) return cuda_fail(e, "zt_backward");
   return ZT_OK;
 }
 

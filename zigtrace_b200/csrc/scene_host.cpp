@@ -397,6 +397,7 @@ void flatten_scene(const zt_scene* s, FlatScene* f) {
     for (int k = 0; k < 9; ++k) d.v[k] = L.shape.p[k];
     for (int k = 0; k < 3; ++k) d.radiance[k] = L.radiance[k];
     d.weight = L.weight;
+    d.material = L.shape.material;
     if (L.shape.kind == ZT_TRIANGLE) {
       d.area = tri_area(L.shape.p);
       double e1[3], e2[3], nrm[3];

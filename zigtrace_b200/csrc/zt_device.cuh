@@ -384,7 +384,7 @@ ZT_D bool sphere_outside(dv3 center, double radius, dv3 origin) { /* light.zig:4
 
 /* Lights.sample, light.zig:120-166. */
 ZT_D bool lights_sample(const DevScene& sc, dv3 origin, Rng& rng, dv3& odir, double& odist, dv3& orad,
-                        double& opdf) {
+                        double& opdf, uint32_t* picked = nullptr) {
   if (sc.n_lights == 0) return false;
   /* pick, light.zig:106-115 */
   const double x = rng_float(rng) * sc.total;
@@ -395,6 +395,7 @@ ZT_D bool lights_sample(const DevScene& sc, dv3 origin, Rng& rng, dv3& odir, dou
     else lo = mid + 1;
   }
   const DLight& L = sc.lights[lo];
+  if (picked) *picked = lo;
   const double select = L.weight / sc.total;
   if (L.kind == kTriangle) {
     const dv3 v0 = L3(L.v), v1 = L3(L.v + 3), v2 = L3(L.v + 6);

@@ -70,7 +70,7 @@ struct ZT_ALIGN(16) DLight {
   double area;       /* triangle only */
   double normal[3];  /* triangle only */
   uint32_t kind;
-  uint32_t pad;
+  uint32_t material; /* the emitter's material (differentiable form) */
 };
 
 struct DCamera {

@@ -203,6 +203,46 @@ def triangle_heavy(seed: int = 0, nx: int = 1000, nz: int = 500, n_ico: int = 20
 TRIANGLE_HEAVY_OPTIONS = Options(width=1920, height=1080, spp=64, max_depth=16, seed=0)
 
 
+# ----------------------------------------------------- differentiable form ----
+def cornell_diff(seed: int = 0, perturb: float = 0.2):
+    """Cornell-style box for the differentiable form: 32 Lambertian materials
+    (floor and back wall 3x3 patches, side walls and ceiling 2x2, two
+    spheres) with albedos U(0.1, 0.9) and 4 emissive quads under the ceiling
+    with radiance U(2, 20) per channel.  Returns (scene, target_colors): the
+    target is every colour scaled by U(1 - perturb, 1 + perturb)."""
+    rng = np.random.default_rng(seed + 500)
+    s = Scene()
+    s.background = Background.solid((0.0, 0.0, 0.0))
+    ids = iter(range(32))
+    for _ in range(32):
+        s.add_material(Material.lambertian(tuple(float(a) for a in rng.uniform(0.1, 0.9, 3))))
+    L = 555.0
+
+    def patches(origin, u, v, nu, nv):
+        for a in range(nu):
+            for b in range(nv):
+                corner = [origin[k] + u[k] * a / nu + v[k] * b / nv for k in range(3)]
+                s.add_quad(corner, [c / nu for c in u], [c / nv for c in v], next(ids))
+
+    patches((0, 0, 0), (L, 0, 0), (0, 0, L), 3, 3)      # floor
+    patches((0, 0, L), (L, 0, 0), (0, L, 0), 3, 3)      # back wall
+    patches((L, 0, 0), (0, L, 0), (0, 0, L), 2, 2)      # x = 555 wall
+    patches((0, 0, 0), (0, L, 0), (0, 0, L), 2, 2)      # x = 0 wall
+    patches((0, L, 0), (L, 0, 0), (0, 0, L), 2, 2)      # ceiling
+    s.add(sphere((185.0, 100.0, 200.0), 100.0, next(ids)))
+    s.add(sphere((380.0, 80.0, 380.0), 80.0, next(ids)))
+    for cx, cz in ((160.0, 160.0), (395.0, 160.0), (160.0, 395.0), (395.0, 395.0)):
+        m = s.add_material(Material.emissive(tuple(float(a) for a in rng.uniform(2.0, 20.0, 3))))
+        s.add_quad((cx - 50.0, 554.0, cz - 40.0), (100.0, 0.0, 0.0), (0.0, 0.0, 80.0), m)  # faces down
+    s.camera = CameraConfig(look_from=(278, 278, -800), look_at=(278, 278, 0), vfov=40)
+    colors = np.array([m["color"] for m in s.materials])
+    target = colors * rng.uniform(1.0 - perturb, 1.0 + perturb, colors.shape)
+    return s, target
+
+
+DIFF_OPTIONS = Options(width=512, height=512, spp=64, max_depth=16, seed=0)
+
+
 # --------------------------------------------------------- batched form ----
 def sphere_field(seed: int, n: int) -> Scene:
     """Ground plane + exactly n r=0.2 spheres on a jittered grid sized to n

@@ -41,7 +41,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--workload", default="triangle_heavy",
-                   choices=["triangle_heavy", "random_spheres", "cornell", "batch"])
+                   choices=["triangle_heavy", "random_spheres", "cornell", "batch", "diff"])
+    p.add_argument("--gd-steps", type=int, default=100, help="gradient-descent steps (--workload diff)")
     p.add_argument("--spp", type=int, default=0, help="override spp (profiling runs)")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size in seconds")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -196,6 +197,8 @@ def b200_arm(args):
 
     if args.workload == "batch":
         return batch_arm(args, world, rank, local_rank, barrier, allmax)
+    if args.workload == "diff":
+        return diff_arm(args, world, rank, local_rank, barrier, allmax)
     scene, o = workload(args.workload, args.spp)
     o.seed = o.seed + rank  # each rank renders its own frame
     scene.build()
@@ -429,6 +432,106 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
     if rank == 0:
         print(json.dumps(line), flush=True)
     batch.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def diff_arm(args, world, rank, local_rank, barrier, allmax):
+    """The differentiable form: Cornell-style box with 32 Lambertian albedos
+    and 4 emitter radiances as parameters, 512x512, 64 spp, L2 loss against
+    a target rendered at parameters perturbed by +/-20%.  Reports forward and
+    backward time through zt_forward / zt_backward (host buffers), the
+    adjoint against central finite differences with common random numbers
+    (h = 1e-3), and a 100-step gradient descent."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import zigtrace_b200 as zt
+    from zigtrace_b200 import scenes
+
+    scene, target = scenes.cornell_diff(seed=rank)
+    scene.build()
+    o = scenes.DIFF_OPTIONS
+    if args.spp:
+        o = zt.Options(o.width, o.height, args.spp, o.max_depth)
+    theta0 = np.array([m["color"] for m in scene.materials])
+    target_img = zt.forward(scene, o, target).pixels
+    samples = o.width * o.height * o.spp
+
+    def fwd(th):
+        return zt.forward(scene, o, th).pixels
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        barrier()
+        return allmax(statistics.mean(ts))
+
+    img = fwd(theta0)
+    d_img = 2.0 * (img - target_img)
+    fwd_s = timed(lambda: fwd(theta0))
+    bwd_s = timed(lambda: zt.backward(scene, o, d_img, theta0))
+    grad = zt.backward(scene, o, d_img, theta0)
+
+    h, errs, fd_vals = 1e-3, [], {}
+    for m, c in ((0, 0), (9, 1), (22, 2), (31, 0), (32, 1), (35, 2)):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[m, c] += h
+        tm[m, c] -= h
+        fd = (((fwd(tp) - target_img) ** 2).sum() - ((fwd(tm) - target_img) ** 2).sum()) / (2 * h)
+        fd_vals[f"{m},{c}"] = [float(grad[m, c]), float(fd)]
+        errs.append(abs(grad[m, c] - fd) / max(abs(fd), 1e-12))
+
+    th = torch.tensor(theta0, dtype=torch.float64)
+    albedo, radiance = th[:32].clone().requires_grad_(), th[32:].clone().requires_grad_()
+    opt = torch.optim.Adam([{"params": [albedo], "lr": 0.01}, {"params": [radiance], "lr": 0.2}])
+    f = zt.render_function()
+    tgt = torch.from_numpy(target_img.copy())
+    losses = []
+    t0 = time.perf_counter()
+    for _ in range(args.gd_steps):
+        opt.zero_grad()
+        loss = ((f.apply(torch.cat([albedo, radiance]), scene, o) - tgt) ** 2).mean()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            albedo.clamp_(0.01, 0.99)
+            radiance.clamp_(min=0.0)
+        losses.append(loss.item())
+    gd_s = time.perf_counter() - t0
+    final = torch.cat([albedo, radiance]).detach().numpy()
+    param_err0 = float(np.abs(theta0 - target).mean())
+    param_err = float(np.abs(final - target).mean())
+
+    line = {
+        "metric": "Msamples/s", "value": round(world * samples / fwd_s / 1e6, 4), "unit": "Msamples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * fwd_s, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": "diff: Cornell-style box, 32 Lambertian albedos + 4 emitter radiances as parameters, "
+                               f"{o.width}x{o.height}, {o.spp} spp, depth {o.max_depth}, L2 loss vs a target at "
+                               "parameters perturbed by +/-20%", "parameters": int(theta0.size)},
+        "forward_ms": round(1e3 * fwd_s, 3), "backward_ms": round(1e3 * bwd_s, 3),
+        "backward_over_forward": round(bwd_s / fwd_s, 3),
+        "adjoint_vs_fd": {"h": h, "max_rel_err": float(max(errs)), "grad_and_fd": fd_vals},
+        "gradient_descent": {"steps": args.gd_steps, "seconds": round(gd_s, 2), "loss_first": losses[0],
+                             "loss_last": losses[-1], "mean_abs_param_err_start": param_err0,
+                             "mean_abs_param_err_end": param_err},
+        "e2e": {"value": round(world * samples / fwd_s / 1e6, 4), "unit": "Msamples/s",
+                "h2d_bytes_per_step": int(theta0.nbytes), "d2h_bytes_per_step": o.width * o.height * 24},
+        "gpu_launches": args.steps, "roofline": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 

@@ -49,12 +49,24 @@ struct zt_wavefront_cache {
   unsigned char key[sizeof(zt::DevScene) + sizeof(zt::RenderParams) + 2 * sizeof(void*)] = {};
 };
 
+/* The per-sample primal radiance of the last zt_forward, with the options
+ * and parameters it was computed for; a zt_backward with the same ones
+ * replays paths against it instead of recomputing the primal. */
+struct zt_diff_cache {
+  double* L = nullptr;
+  size_t cap = 0; /* doubles */
+  bool valid = false;
+  zt_options opts{};
+  std::vector<double> theta;
+};
+
 struct zt_device_buffers {
   int device = -1;
   void* block = nullptr;           /* all scene arrays */
   unsigned int* counter = nullptr; /* work counter of the persistent grid */
   DevScene view;
   zt_wavefront_cache wf;
+  zt_diff_cache diff;
 };
 
 namespace zt {
@@ -80,6 +92,7 @@ void release_device(zt_scene* s) {
   if (d->wf.exec) cudaGraphExecDestroy(d->wf.exec);
   if (d->wf.done) cudaEventDestroy(d->wf.done);
   cudaFree(d->wf.block);
+  cudaFree(d->diff.L);
   cudaFree(d->block);
   cudaFree(d->counter);
   if (d->device >= 0 && d->device != cur) cudaSetDevice(cur);
@@ -817,7 +830,8 @@ namespace zt {
 template <int BS>
 __global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, RenderParams p,
                                                              const double* __restrict__ theta,
-                                                             double* __restrict__ out, unsigned int* __restrict__ counter) {
+                                                             double* __restrict__ out, double* __restrict__ sample_L,
+                                                             unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
@@ -835,8 +849,14 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, Rend
       const double t = ((double)y + rng_float(rng)) / (double)p.height;
       dv3 ro, rd;
       camera_ray(p.cam, s, t, rng, ro, rd);
-      const dv3 c = trace_diff<false>(sc, theta, ro, rd, rng, p.max_depth, p.use_nee != 0, V(0, 0, 0), V(0, 0, 0),
-                                      nullptr);
+      const dv3 c = trace_diff(sc, theta, ro, rd, rng, p.max_depth, p.use_nee != 0, false, V(0, 0, 0), V(0, 0, 0),
+                               nullptr, false);
+      if (sample_L) { /* the primal radiance of every sample, kept for zt_backward */
+        double* q = sample_L + 3 * (i * p.width * p.height + pix);
+        q[0] = c.x;
+        q[1] = c.y;
+        q[2] = c.z;
+      }
       if (visfinite(c)) sum = sum + c;
     }
     const dv3 px = vscale(sum, 1.0 / (double)p.spp);
@@ -855,11 +875,12 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, Ren
                                                               const double* __restrict__ theta,
                                                               const double* __restrict__ dimg, double* grad,
                                                               uint32_t n_params, int use_smem,
+                                                              const double* __restrict__ sample_L,
                                                               unsigned int* __restrict__ counter) {
   extern __shared__ double sgrad[];
-  double* g = use_smem ? sgrad : grad;
+  double* g = use_smem ? sgrad + (threadIdx.x >> 5) * n_params : grad; /* a slice per warp */
   if (use_smem) {
-    for (uint32_t i = threadIdx.x; i < n_params; i += BS) sgrad[i] = 0.0;
+    for (uint32_t i = threadIdx.x; i < n_params * (BS / 32); i += BS) sgrad[i] = 0.0;
     __syncthreads();
   }
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
@@ -881,32 +902,68 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, Ren
       const double t = ((double)y + rng_float(rng)) / (double)p.height;
       dv3 ro, rd;
       camera_ray(p.cam, s, t, rng, ro, rd);
-      Rng replay = rng;
-      const dv3 L = trace_diff<false>(sc, theta, ro, rd, rng, p.max_depth, p.use_nee != 0, V(0, 0, 0), V(0, 0, 0),
-                                      nullptr);
-      if (visfinite(L)) trace_diff<true>(sc, theta, ro, rd, replay, p.max_depth, p.use_nee != 0, L, adj, g);
+      const Rng start = rng;
+      dv3 L = V(0, 0, 0);
+      int first_pass = 0;
+      if (sample_L) { /* the forward kept the primal radiance: replay only */
+        L = L3(sample_L + 3 * (i * p.width * p.height + pix));
+        first_pass = 1;
+        if (!visfinite(L)) { /* dropped by the forward (render.zig:142): advance the stream only */
+          Rng r = start;
+          trace_diff(sc, theta, ro, rd, r, p.max_depth, p.use_nee != 0, false, L, adj, g, use_smem);
+          rng = r;
+          continue;
+        }
+      }
+#pragma unroll 1
+      for (int pass = first_pass; pass < 2; ++pass) { /* primal, then replay from the same stream state */
+        Rng r = start;
+        const dv3 v = trace_diff(sc, theta, ro, rd, r, p.max_depth, p.use_nee != 0, pass == 1, L, adj, g, use_smem);
+        if (pass == 0) {
+          L = v;
+          if (!visfinite(L)) { /* dropped by the forward (render.zig:142): no gradient */
+            rng = r;
+            break;
+          }
+        } else {
+          rng = r; /* the replay draws exactly what the primal drew */
+        }
+      }
     }
   }
-  if (use_smem) {
+  if (use_smem) { /* sum the warps' slices, then one global add per parameter and block */
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n_params; i += BS)
-      if (sgrad[i] != 0.0) atomicAdd(grad + i, sgrad[i]);
+    for (uint32_t i = threadIdx.x; i < n_params; i += BS) {
+      double acc = 0.0;
+      for (int wi = 0; wi < BS / 32; ++wi) acc += sgrad[wi * n_params + i];
+      if (acc != 0.0) atomicAdd(grad + i, acc);
+    }
   }
 }
 
-/* theta on the device: the caller's colours, or the scene's own. */
-static zt_status upload_theta(const zt_scene* s, const double* colors, double** d_theta) {
-  const size_t n = s->materials.size() * 3;
-  std::vector<double> th(n > 0 ? n : 3, 0.0);
+/* theta on the host: the caller's colours, or the scene's own. */
+static std::vector<double> theta_host(const zt_scene* s, const double* colors) {
+  std::vector<double> th(s->materials.size() * 3, 0.0);
   for (size_t m = 0; m < s->materials.size(); ++m) {
     const zt_vec3& c = s->materials[m].color;
     th[3 * m + 0] = colors ? colors[3 * m + 0] : c.x;
     th[3 * m + 1] = colors ? colors[3 * m + 1] : c.y;
     th[3 * m + 2] = colors ? colors[3 * m + 2] : c.z;
   }
-  ZT_CUDA(cudaMalloc((void**)d_theta, th.size() * sizeof(double)), "allocate parameters");
-  ZT_CUDA(cudaMemcpy(*d_theta, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice), "upload parameters");
+  return th;
+}
+
+static zt_status upload_theta(const std::vector<double>& th, double** d_theta) {
+  const size_t n = th.empty() ? 3 : th.size();
+  ZT_CUDA(cudaMalloc((void**)d_theta, n * sizeof(double)), "allocate parameters");
+  if (!th.empty())
+    ZT_CUDA(cudaMemcpy(*d_theta, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice), "upload parameters");
   return ZT_OK;
+}
+
+static bool same_render(const zt_options& a, const zt_options& b) {
+  return a.width == b.width && a.height == b.height && a.spp == b.spp && a.max_depth == b.max_depth &&
+         a.seed == b.seed && a.light_sampling == b.light_sampling;
 }
 
 }  // namespace zt
@@ -920,23 +977,41 @@ zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, dou
   if ((rc = upload(s)) != ZT_OK) return rc;
   const RenderParams p = make_params(s, o);
   const size_t bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  zt_diff_cache& cache = s->device->diff;
+  cache.valid = false;
   if (p.max_depth == 0) {
     memset(out, 0, bytes);
     return ZT_OK;
   }
+  const std::vector<double> th = theta_host(s, colors);
   double *d_theta = nullptr, *d_out = nullptr;
-  if ((rc = upload_theta(s, colors, &d_theta)) != ZT_OK) return rc;
+  if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
+  /* keep every sample's primal radiance for a following zt_backward (24 bytes
+   * per sample); if that memory is not available the backward recomputes it */
+  const size_t n_l = (size_t)(p.width * p.height * p.spp) * 3;
+  if (cache.cap < n_l) {
+    cudaFree(cache.L);
+    cache.L = nullptr;
+    cache.cap = 0;
+    if (cudaMalloc((void**)&cache.L, n_l * sizeof(double)) == cudaSuccess) cache.cap = n_l;
+    else cudaGetLastError();
+  }
   cudaError_t e = cudaMalloc((void**)&d_out, bytes);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
   if (e == cudaSuccess) {
     k_forward_diff<128><<<persistent_grid(k_forward_diff<128>, 128, p.width * p.height), 128>>>(
-        launch_view(s), p, d_theta, d_out, s->device->counter);
+        launch_view(s), p, d_theta, d_out, cache.L, s->device->counter);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
   cudaFree(d_theta);
   cudaFree(d_out);
   if (e != cudaSuccess) return cuda_fail(e, "zt_forward");
+  if (cache.L) {
+    cache.valid = true;
+    cache.opts = *o;
+    cache.theta = th;
+  }
   return ZT_OK;
 }
 
@@ -950,24 +1025,27 @@ zt_status zt_backward(zt_scene* s, const zt_options* o, const double* colors, co
   const uint32_t n_params = (uint32_t)(s->materials.size() * 3);
   memset(d_colors, 0, n_params * sizeof(double));
   if (p.max_depth == 0 || n_params == 0) return ZT_OK;
+  const std::vector<double> th = theta_host(s, colors);
+  const zt_diff_cache& cache = s->device->diff;
+  const double* sample_L = (cache.valid && same_render(cache.opts, *o) && cache.theta == th) ? cache.L : nullptr;
   const size_t img_bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
   double *d_theta = nullptr, *d_img = nullptr, *d_grad = nullptr;
-  if ((rc = upload_theta(s, colors, &d_theta)) != ZT_OK) return rc;
+  if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
   cudaError_t e = cudaMalloc((void**)&d_img, img_bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&d_grad, n_params * sizeof(double));
   if (e == cudaSuccess) e = cudaMemcpy(d_img, d_image, img_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(d_grad, 0, n_params * sizeof(double));
   if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
   if (e == cudaSuccess) {
-    const size_t smem = (size_t)n_params * sizeof(double);
-    const int use_smem = smem <= 32 * 1024 ? 1 : 0;
+    const size_t smem = (size_t)n_params * sizeof(double) * (128 / 32); /* one slice per warp */
+    const int use_smem = smem <= 48 * 1024 ? 1 : 0;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backward_diff<128>, 128, use_smem ? smem : 0);
     uint64_t blocks = (uint64_t)sm_count() * (per_sm > 0 ? per_sm : 1);
     const uint64_t need = (p.width * p.height + 127) / 128;
     if (blocks > need) blocks = need;
-    k_backward_diff<128><<<(unsigned)blocks, 128, use_smem ? smem : 0>>>(launch_view(s), p, d_theta, d_img, d_grad,
-                                                                         n_params, use_smem, s->device->counter);
+    k_backward_diff<128><<<(unsigned)blocks, 128, use_smem ? smem : 0>>>(
+        launch_view(s), p, d_theta, d_img, d_grad, n_params, use_smem, sample_L, s->device->counter);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(d_colors, d_grad, n_params * sizeof(double), cudaMemcpyDeviceToHost);

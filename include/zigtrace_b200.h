@@ -130,6 +130,13 @@ zt_status zt_scene_upload_bytes(zt_scene* scene, uint64_t* bytes);
 /* render.render into a caller-owned host buffer of width*height*3 doubles,
  * row-major, top row first.  Uploads the scene if it is not resident. */
 zt_status zt_render(zt_scene* scene, const zt_options* opts, double* out_rgb);
+/* render.render restricted to image rows [row_begin, row_end) of the
+ * width x height image: same camera, same per-pixel RNG streams, so the band
+ * equals those rows of zt_render's image.  Used to shard one image across
+ * devices (each renders a band; the bands are gathered).  out has
+ * (row_end - row_begin)*width*3 doubles. */
+zt_status zt_render_rows(zt_scene* scene, const zt_options* opts, uint64_t row_begin, uint64_t row_end,
+                         double* out_rgb);
 /* The same with explicit device choices (cfg may be NULL). */
 zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                        double* out_rgb);

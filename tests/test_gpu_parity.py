@@ -124,6 +124,38 @@ def test_render_device_on_torch_stream_matches_host_render(mode):
     assert out.cpu().numpy().reshape(-1, 3).tobytes() == want.tobytes()
 
 
+def test_row_bands_reassemble_the_image():
+    from zigtrace_b200 import sharding
+    scene = scenes.random_spheres().build()
+    o = zt.Options(200, 113, 3, 50, seed=4)
+    full = zt.render(scene, o).pixels
+    bands = sharding.row_bands(o.height, 3, np.linspace(1, 3, o.height))
+    parts = [sharding.render_rows(scene, o, a, b) for a, b in bands]
+    assert np.concatenate(parts).tobytes() == full.tobytes()
+    with pytest.raises(zt.ZigtraceError):
+        sharding.render_rows(scene, o, 50, 40)
+
+
+def test_render_sharded_over_nccl_single_rank():
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from zigtrace_b200 import sharding
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        scene = scenes.cornell().build()
+        o = zt.Options(64, 40, 2, 16)
+        img = sharding.render_sharded(scene, o)
+        assert img.tobytes() == zt.render(scene, o).pixels.tobytes()
+    finally:
+        dist.destroy_process_group()
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_edge_options(mode):
     scene = K.demo_scene().build()

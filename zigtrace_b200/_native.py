@@ -72,6 +72,7 @@ SIGNATURES = {
     "zt_scene_upload_bytes": (_i32, [_P, C.POINTER(_u64)]),
     "zt_render": (_i32, [_P, _P, _P]),
     "zt_render_ex": (_i32, [_P, _P, _P, _P]),
+    "zt_render_rows": (_i32, [_P, _P, _u64, _u64, _P]),
     "zt_render_device": (_i32, [_P, _P, _P, _P, _P]),
     "zt_render_debug": (_i32, [_P, _P, _P, _P]),
     "zt_render_noalloc": (_i32, [_P, _P, _P, _P]),

@@ -215,6 +215,8 @@ static RenderParams make_params(const zt_scene* s, const zt_options* o) {
   p.max_depth = o->max_depth;
   p.seed = o->seed;
   p.use_nee = (o->light_sampling && !s->lights.empty()) ? 1u : 0u; /* render.zig:62 */
+  p.row0 = 0;
+  p.rows = o->height;
   p.pad = 0;
   return p;
 }
@@ -241,9 +243,10 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
   }
   if (!kAux) {
     const dv3 px = vscale(sum, inv_spp);
-    out[3 * pix + 0] = px.x;
-    out[3 * pix + 1] = px.y;
-    out[3 * pix + 2] = px.z;
+    const uint64_t o = pix - p.row0 * p.width; /* output starts at the band's first row */
+    out[3 * o + 0] = px.x;
+    out[3 * o + 1] = px.y;
+    out[3 * o + 2] = px.z;
   }
 }
 
@@ -255,15 +258,16 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
 template <int BS>
 __global__ void __launch_bounds__(BS, 896 / BS) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
                                                             unsigned int* __restrict__ counter) {
-  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
+  const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
     unsigned tile = 0;
     if (lane == 0) tile = atomicAdd(counter, 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) return;
-    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
-    if (x < p.width && y < p.height) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
+    if (x < p.width && y < row_end) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
   }
 }
 
@@ -752,6 +756,32 @@ zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cf
 }
 
 zt_status zt_render(zt_scene* s, const zt_options* o, double* out) { return zt_render_ex(s, o, nullptr, out); }
+
+zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end, double* out) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_rows: NULL output");
+  if (row_begin >= row_end || row_end > o->height)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_rows: need row_begin < row_end <= height");
+  if ((rc = upload(s)) != ZT_OK) return rc;
+  RenderParams p = make_params(s, o); /* camera and RNG streams of the whole image */
+  p.row0 = row_begin;
+  p.rows = row_end - row_begin;
+  const size_t bytes = (size_t)(p.rows * p.width * 3) * sizeof(double);
+  if (p.max_depth == 0) {
+    memset(out, 0, bytes);
+    return ZT_OK;
+  }
+  double* d_out = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
+  rc = launch_mega(s, p, 0, d_out, 0);
+  if (rc == ZT_OK) {
+    const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");
+  }
+  cudaFree(d_out);
+  return rc;
+}
 
 zt_status zt_render_debug(zt_scene* s, const zt_options* o, int32_t* first_prim, uint32_t* path_len) {
   zt_status rc = check_render_args(s, o);

@@ -105,6 +105,7 @@ struct DevScene {
 struct RenderParams {
   DCamera cam;
   uint64_t width, height, spp, max_depth, seed;
+  uint64_t row0, rows; /* the band of image rows rendered; output row 0 is image row row0 */
   uint32_t use_nee;  /* light_sampling && !lights.isEmpty() */
   uint32_t pad;
 };

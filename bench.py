@@ -304,7 +304,7 @@ def b200_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
-                   "mode": ["auto", "megakernel", "wavefront"][args.mode],
+                   "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][args.mode],
                    "sharding": "one frame per rank (seed = rank), no collective"},
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
     }

@@ -77,8 +77,14 @@ typedef struct { zt_vec3 bmin, bmax; uint32_t first, count; } zt_bvh_node;
 /* Light, src/light.zig:30-35 (host copy, for inspection). */
 typedef struct { zt_shape shape; zt_vec3 radiance; double weight; } zt_light;
 
-/* Device-side execution choices; zero-initialised means "defaults". */
-enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2 };
+/* Device-side execution choices; zero-initialised means "defaults".
+ * MEGAKERNEL: one persistent kernel, each warp renders an 8x4 pixel tile
+ * sample by sample.  WAVEFRONT: per-bounce kernels over ray queues in a CUDA
+ * graph.  MEGAKERNEL_REGEN: the megakernel with per-lane path regeneration
+ * (a lane whose path ends starts its next sample at once); faster on closed
+ * scenes with long paths.  AUTO is MEGAKERNEL.  All modes give bit-identical
+ * images. */
+enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_MEGAKERNEL_REGEN = 3 };
 typedef struct {
   uint32_t mode;           /* ZT_MODE_* */
   uint32_t block_size;     /* threads per block, 0 = default */

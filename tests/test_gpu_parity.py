@@ -16,7 +16,8 @@ import zigtrace_b200 as zt
 from zigtrace_b200 import scenes
 
 pytestmark = pytest.mark.gpu
-MODES = [pytest.param(zt.MODE_MEGAKERNEL, id="mega"), pytest.param(zt.MODE_WAVEFRONT, id="wavefront")]
+MODES = [pytest.param(zt.MODE_MEGAKERNEL, id="mega"), pytest.param(zt.MODE_WAVEFRONT, id="wavefront"),
+         pytest.param(zt.MODE_MEGAKERNEL_REGEN, id="regen")]
 
 DEBUG_CASES = {
     "demo": (K.demo_scene, dict(width=48, height=32, max_depth=8)),

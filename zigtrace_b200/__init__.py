@@ -10,7 +10,7 @@ radiance path, behind a mirror of the reference library API.
     rgb = img.to_rgb8(zt.Output(tonemap="aces"))
 """
 from .api import (  # noqa: F401
-    DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, PLANE, SPHERE, TRIANGLE,
+    DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, PLANE, SPHERE, TRIANGLE,
     Background, Batch, CameraConfig, GpuConfig, Image, Material, Options, Output, Scene, Settings, ZigtraceError,
     backward, forward, plane, render, render_batch, render_debug, render_device, render_function, rng_streams,
     set_colors, sphere, triangle, write_ppm)

@@ -1,7 +1,7 @@
 """Autotuner for the device execution choices.
 
-For a render it times the megakernel at block sizes 64/128/256 and the
-wavefront form; for a batch it times block sizes 64/128/256 with the renders
+For a render it times the megakernel at block sizes 64/128/256, the
+megakernel with path regeneration and the wavefront form; for a batch it times block sizes 64/128/256 with the renders
 in the given order or largest first.  Every candidate renders identical
 pixels (the choice only changes scheduling), so the fastest one is kept.
 Results are cached per (GPU, scene class) in a JSON file, by default
@@ -16,10 +16,11 @@ import statistics
 from pathlib import Path
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
-from .api import MODE_MEGAKERNEL, MODE_WAVEFRONT, Batch, GpuConfig, Options, Scene, render_device
+from .api import MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, Batch, GpuConfig, Options, Scene, render_device
 
 SINGLE_CANDIDATES: List[Tuple[int, int, int]] = [  # (mode, block_size, queue_capacity)
-    (MODE_MEGAKERNEL, 64, 0), (MODE_MEGAKERNEL, 128, 0), (MODE_MEGAKERNEL, 256, 0), (MODE_WAVEFRONT, 128, 0)]
+    (MODE_MEGAKERNEL, 64, 0), (MODE_MEGAKERNEL, 128, 0), (MODE_MEGAKERNEL, 256, 0),
+    (MODE_MEGAKERNEL_REGEN, 128, 0), (MODE_WAVEFRONT, 128, 0)]
 BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)]
 
 

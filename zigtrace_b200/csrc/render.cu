@@ -271,6 +271,110 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_render_mega(DevScene sc, Rende
   }
 }
 
+/* render_pixel with per-lane path regeneration: a lane whose path ends starts
+ * its pixel's next sample at once instead of waiting at the sample boundary
+ * for the longest path of its warp.  Per lane the operations and RNG draws
+ * are render_pixel's and trace_with's in the same order (render.zig:61-102,
+ * 133-144), so the pixel is bit-identical; only the warp's schedule changes.
+ * All 32 lanes of the warp must call it (lanes outside the image with
+ * valid = false).  Pays off when path lengths vary widely within a warp
+ * (closed scenes such as the Cornell box); on open scenes with short paths
+ * the nested form is faster. */
+__device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const RenderParams& p, uint64_t x, uint64_t y,
+                                                   bool valid, double* __restrict__ out) {
+  const double w = (double)p.width, h = (double)p.height;
+  const bool use_nee = p.use_nee != 0;
+  Rng rng = rng_for_stream(p.seed, valid ? y * p.width + x : 0);
+  dv3 sum = V(0, 0, 0);
+  uint64_t sample = 0, depth = 0;
+  bool done = !valid, fresh = valid;
+  dv3 ro = V(0, 0, 0), rd = V(0, 0, 0), radiance = V(0, 0, 0), throughput = V(1, 1, 1), prev_origin = V(0, 0, 0);
+  double prev_pdf = 0;
+  for (;;) {
+    if (fresh) { /* render.zig:138-140: the next sample's camera ray */
+      fresh = false;
+      if (sample == p.spp) {
+        done = true;
+      } else {
+        const double s = ((double)x + rng_float(rng)) / w;
+        const double t = ((double)y + rng_float(rng)) / h;
+        camera_ray(p.cam, s, t, rng, ro, rd);
+        radiance = V(0, 0, 0);
+        throughput = V(1, 1, 1);
+        prev_origin = V(0, 0, 0);
+        prev_pdf = 0;
+        depth = 0;
+      }
+    }
+    if (__all_sync(0xffffffffu, done)) break;
+    if (done) continue;
+    /* one iteration of traceWith's bounce loop */
+    bool end = depth >= p.max_depth;
+    if (!end) {
+      Hit hit;
+      if (!scene_intersect<false>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
+        radiance = radiance + vmul(throughput, background_radiance(sc.bg, rd));
+        end = true;
+      } else {
+        const DMat& mat = sc.mats[hit.material];
+        const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
+        if (vmaxc(le) > 0) {
+          const double wt = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, prev_origin, hit.point)) : 1.0;
+          radiance = radiance + vscale(vmul(throughput, le), wt);
+        }
+        if (mat.kind == kLambertian && use_nee)
+          radiance = radiance + vmul(throughput, direct_light(sc, L3(mat.color), hit, rng));
+        dv3 atten, sd;
+        if (!material_scatter(mat, rd, hit, rng, atten, sd)) {
+          end = true;
+        } else {
+          throughput = vmul(throughput, atten);
+          prev_pdf = (use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
+          prev_origin = hit.point;
+          ro = hit.point;
+          rd = sd;
+          if (depth + 1 >= kRouletteDepth) {
+            const double pr = fmin(vmaxc(throughput), 0.95);
+            if (pr <= 0 || rng_float(rng) >= pr) end = true;
+            else throughput = vdiv(throughput, pr);
+          }
+          depth += 1;
+          if (depth >= p.max_depth) end = true;
+        }
+      }
+    }
+    if (end) { /* render.zig:141-142 */
+      if (visfinite(radiance)) sum = sum + radiance;
+      ++sample;
+      fresh = true;
+    }
+  }
+  if (valid) {
+    const dv3 px = vscale(sum, 1.0 / (double)p.spp);
+    const uint64_t o = (y - p.row0) * p.width + x;
+    out[3 * o + 0] = px.x;
+    out[3 * o + 1] = px.y;
+    out[3 * o + 2] = px.z;
+  }
+}
+
+/* The megakernel's tile loop over render_pixel_regen. */
+template <int BS>
+__global__ void __launch_bounds__(BS, 896 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
+                                                             unsigned int* __restrict__ counter) {
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
+  const uint64_t row_end = p.row0 + p.rows;
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= tiles) return;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
+    render_pixel_regen(sc, p, x, y, x < p.width && y < row_end, out);
+  }
+}
+
 /* One render of a batch: its scene view, parameters, output and the index
  * of its first tile in the batch-wide tile numbering. */
 struct BatchItem {
@@ -535,22 +639,25 @@ static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
 
 template <int BS>
 static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
-                           cudaStream_t stream) {
-  k_render_mega<BS><<<persistent_grid(k_render_mega<BS>, BS, p.width * p.height), BS, 0, stream>>>(v, p, d_out,
-                                                                                                  counter);
+                           bool regen, cudaStream_t stream) {
+  const uint64_t npix = p.width * p.rows;
+  if (regen)
+    k_render_regen<BS><<<persistent_grid(k_render_regen<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
+  else
+    k_render_mega<BS><<<persistent_grid(k_render_mega<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
 }
 
 static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
 
-static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out,
+static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out, bool regen,
                              cudaStream_t stream) {
   zt_device_buffers* d = s->device;
   ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
   const DevScene v = launch_view(s);
-  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, stream);
-  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, stream);
-  else launch_mega_bs<128>(v, p, d_out, d->counter, stream);
-  ZT_CUDA(cudaGetLastError(), "launch k_render_mega");
+  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, regen, stream);
+  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, regen, stream);
+  else launch_mega_bs<128>(v, p, d_out, d->counter, regen, stream);
+  ZT_CUDA(cudaGetLastError(), regen ? "launch k_render_regen" : "launch k_render_mega");
   return ZT_OK;
 }
 
@@ -677,10 +784,10 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   }
   const uint32_t mode = cfg ? cfg->mode : ZT_MODE_AUTO;
   if (mode == ZT_MODE_WAVEFRONT) return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
-  if (mode > ZT_MODE_WAVEFRONT) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
+  if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
-  return launch_mega(s, p, bs, d_out, stream);
+  return launch_mega(s, p, bs, d_out, mode == ZT_MODE_MEGAKERNEL_REGEN, stream);
 }
 
 /* Error word of the last wavefront launch (after the stream is idle). */
@@ -774,7 +881,7 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   }
   double* d_out = nullptr;
   ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
-  rc = launch_mega(s, p, 0, d_out, 0);
+  rc = launch_mega(s, p, 0, d_out, false, 0);
   if (rc == ZT_OK) {
     const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");

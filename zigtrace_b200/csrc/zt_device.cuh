@@ -202,27 +202,31 @@ ZT_D void prim_hit(const DPrim& p, dv3 o, dv3 d, double t, Hit& h) {
 /* --------------------------------------------------------- Traversal ---- */
 /* Slab test of one box, aabb.zig:68-83.  The reference returns early once
  * hi < lo; lo only grows and hi only shrinks afterwards, so testing once at
- * the end is the same predicate, and `if (t0 > lo) lo = t0` equals
- * fmax(lo, t0) including the NaN case (0 * inf leaves lo unchanged). */
+ * the end is the same predicate.  The updates keep the reference's compares
+ * (a NaN plane distance, 0 * inf, leaves lo and hi unchanged): written as
+ * compare-and-select they measured faster than f64 fmax/fmin. */
 ZT_D bool slab(const double* lo3, const double* hi3, dv3 o, dv3 inv, double tmin, double tmax, double& tout) {
   double lo = tmin, hi = tmax;
   {
     double t0 = (lo3[0] - o.x) * inv.x, t1 = (hi3[0] - o.x) * inv.x;
     const bool sw = inv.x < 0;
-    lo = fmax(lo, sw ? t1 : t0);
-    hi = fmin(hi, sw ? t0 : t1);
+    const double n = sw ? t1 : t0, f = sw ? t0 : t1;
+    lo = n > lo ? n : lo;
+    hi = f < hi ? f : hi;
   }
   {
     double t0 = (lo3[1] - o.y) * inv.y, t1 = (hi3[1] - o.y) * inv.y;
     const bool sw = inv.y < 0;
-    lo = fmax(lo, sw ? t1 : t0);
-    hi = fmin(hi, sw ? t0 : t1);
+    const double n = sw ? t1 : t0, f = sw ? t0 : t1;
+    lo = n > lo ? n : lo;
+    hi = f < hi ? f : hi;
   }
   {
     double t0 = (lo3[2] - o.z) * inv.z, t1 = (hi3[2] - o.z) * inv.z;
     const bool sw = inv.z < 0;
-    lo = fmax(lo, sw ? t1 : t0);
-    hi = fmin(hi, sw ? t0 : t1);
+    const double n = sw ? t1 : t0, f = sw ? t0 : t1;
+    lo = n > lo ? n : lo;
+    hi = f < hi ? f : hi;
   }
   tout = lo;
   return !(hi < lo);

@@ -279,15 +279,22 @@ ZT_D int32_t scene_query_rt(const DevScene& sc, dv3 o, dv3 d, double tmin, doubl
   double t;
   const dv3 inv = V(1.0 / d.x, 1.0 / d.y, 1.0 / d.z); /* aabb.zig:86-88 */
   if (sc.has_root && slab(sc.root_lo, sc.root_hi, o, inv, tmin, closest, t)) {
-    /* Nearest-first stack traversal, bvh.zig:94-124: one pop per step. */
+    /* Nearest-first stack traversal, bvh.zig:94-124.  The nearer child of a
+     * two-hit node stays in registers as the next entry instead of being
+     * pushed and popped at once: the same visiting order and pop check. */
     StackEntry stack[kStackSize];
-    stack[0].first = sc.root_first;
-    stack[0].count = sc.root_count;
-    stack[0].t = t;
-    int sp = 1;
-    while (sp > 0) {
-      --sp;
-      const StackEntry e = stack[sp];
+    StackEntry e;
+    e.first = sc.root_first;
+    e.count = sc.root_count;
+    e.t = t;
+    bool have = true;
+    int sp = 0;
+    for (;;) {
+      if (!have) {
+        if (sp == 0) break;
+        e = stack[--sp];
+      }
+      have = false;
       if (e.t > closest) continue; /* bvh.zig:97 */
       if (e.count > 0) {
         for (uint32_t k = e.first; k < e.first + e.count; ++k) {
@@ -310,20 +317,21 @@ ZT_D int32_t scene_query_rt(const DevScene& sc, dv3 o, dv3 d, double tmin, doubl
       double tl, tr;
       const bool hl = slab(lo0, hi0, o, inv, tmin, closest, tl);
       const bool hr = slab(lo1, hi1, o, inv, tmin, closest, tr);
-      if (hl && hr) { /* push the farther child first (bvh.zig:111-116) */
+      if (hl && hr) { /* push the farther child; the nearer one is popped next (bvh.zig:111-116) */
         const bool near_left = tl <= tr;
         stack[sp].first = near_left ? pc.y : pc.x;
         stack[sp].count = near_left ? pc.w : pc.z;
         stack[sp].t = near_left ? tr : tl;
-        stack[sp + 1].first = near_left ? pc.x : pc.y;
-        stack[sp + 1].count = near_left ? pc.z : pc.w;
-        stack[sp + 1].t = near_left ? tl : tr;
-        sp += 2;
-      } else if (hl || hr) {
-        stack[sp].first = hl ? pc.x : pc.y;
-        stack[sp].count = hl ? pc.z : pc.w;
-        stack[sp].t = hl ? tl : tr;
         sp += 1;
+        e.first = near_left ? pc.x : pc.y;
+        e.count = near_left ? pc.z : pc.w;
+        e.t = near_left ? tl : tr;
+        have = true;
+      } else if (hl || hr) {
+        e.first = hl ? pc.x : pc.y;
+        e.count = hl ? pc.z : pc.w;
+        e.t = hl ? tl : tr;
+        have = true;
       }
     }
   }

@@ -637,11 +637,14 @@ static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
   return (unsigned)(blocks > 0 ? blocks : 1);
 }
 
+/* Megakernel variants: the nested kernel and path regeneration. */
+enum MegaVariant { kMegaNested = 0, kMegaRegen = 1 };
+
 template <int BS>
 static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
-                           bool regen, cudaStream_t stream) {
+                           MegaVariant variant, cudaStream_t stream) {
   const uint64_t npix = p.width * p.rows;
-  if (regen)
+  if (variant == kMegaRegen)
     k_render_regen<BS><<<persistent_grid(k_render_regen<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
   else
     k_render_mega<BS><<<persistent_grid(k_render_mega<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
@@ -649,15 +652,15 @@ static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_o
 
 static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
 
-static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out, bool regen,
-                             cudaStream_t stream) {
+static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out,
+                             MegaVariant variant, cudaStream_t stream) {
   zt_device_buffers* d = s->device;
   ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
   const DevScene v = launch_view(s);
-  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, regen, stream);
-  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, regen, stream);
-  else launch_mega_bs<128>(v, p, d_out, d->counter, regen, stream);
-  ZT_CUDA(cudaGetLastError(), regen ? "launch k_render_regen" : "launch k_render_mega");
+  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, variant, stream);
+  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, variant, stream);
+  else launch_mega_bs<128>(v, p, d_out, d->counter, variant, stream);
+  ZT_CUDA(cudaGetLastError(), "launch the megakernel");
   return ZT_OK;
 }
 
@@ -787,7 +790,8 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
-  return launch_mega(s, p, bs, d_out, mode == ZT_MODE_MEGAKERNEL_REGEN, stream);
+  const MegaVariant variant = mode == ZT_MODE_MEGAKERNEL_REGEN ? kMegaRegen : kMegaNested;
+  return launch_mega(s, p, bs, d_out, variant, stream);
 }
 
 /* Error word of the last wavefront launch (after the stream is idle). */
@@ -881,7 +885,7 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   }
   double* d_out = nullptr;
   ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
-  rc = launch_mega(s, p, 0, d_out, false, 0);
+  rc = launch_mega(s, p, 0, d_out, kMegaNested, 0);
   if (rc == ZT_OK) {
     const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");

@@ -32,6 +32,11 @@ sys.path.insert(0, str(ROOT))
 
 FP64_LANES_PER_SM = 64
 NOMINAL_SM_MHZ = 1965.0
+# DRAM bytes (read + write) per sample of the megakernel, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one 8-spp launch of the
+# workload, --clock-control none) and scaled by samples per launch: traffic
+# grows with the samples traced.  Workloads without a capture report null.
+NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 3.347888e9 / (1920 * 1080 * 8)}
 
 
 def parse_args():
@@ -287,7 +292,10 @@ def b200_arm(args):
         bytes_per_launch = work["bytes"] * samples
         roofline = {
             "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
-            "frac": round(achieved / peak, 4), "traffic": None,
+            "frac": round(achieved / peak, 4),
+            "traffic": (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
+                        if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
+            "traffic_note": "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
             "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
                            "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
             "algorithmic_flop_per_sample": round(work["flop"], 1),
@@ -468,13 +476,13 @@ def diff_arm(args, world, rank, local_rank, barrier, allmax):
         torch.cuda.synchronize()
         barrier()
         ts = []
-        for _ in range(args.steps):
+        for _ in range(max(args.steps, 5)):  # host-timed calls: the median of at least 5 resists host jitter
             t0 = time.perf_counter()
             fn()
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t0)
         barrier()
-        return allmax(statistics.mean(ts))
+        return allmax(statistics.median(ts))
 
     img = fwd(theta0)
     d_img = 2.0 * (img - target_img)

@@ -114,6 +114,14 @@ zt_status zt_scene_set_background(zt_scene* scene, const zt_background* bg);
 /* Scene.build: binned-SAH BVH and the emitter table, on the host
  * (bvh.zig:41-67, light.zig:68-94). */
 zt_status zt_scene_build(zt_scene* scene);
+/* Scene.build with the BVH built on the current CUDA device: the same nodes,
+ * primitive order and numbering as zt_scene_build (bvh.zig:41-262), node
+ * bounds equal up to the sign of zero.  Scenes that need the reference's
+ * median split (more than 4 primitives whose centroids coincide, or bounds
+ * without area) or hold non-finite coordinates are built on the host;
+ * *used_device (may be NULL) is 1 when the device built the BVH.
+ * *build_ms (may be NULL) is the device time of the build. */
+zt_status zt_scene_build_device(zt_scene* scene, uint32_t* used_device, double* build_ms);
 
 /* ---- Inspection (Scene fields, Bvh, Lights) --------------------------- */
 zt_status zt_scene_counts(const zt_scene* scene, uint64_t* n_materials, uint64_t* n_bounded,
@@ -227,6 +235,35 @@ zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, ui
  * to u8, on the host.  rgb_out has n_pixels*3 bytes. */
 zt_status zt_image_to_rgb8(const double* pixels, uint64_t n_pixels, uint32_t tonemap, double gamma,
                            double exposure, uint8_t* rgb_out);
+/* Image.toRgb8 on the device: d_pixels (n_pixels*3 f64) and d_rgb_out
+ * (n_pixels*3 bytes) are device pointers; asynchronous on `stream` (a
+ * cudaStream_t, NULL for the default stream).  The same bytes as
+ * zt_image_to_rgb8 except where pow() of the two math libraries rounds a
+ * value to opposite sides of a u8 rounding boundary (at most 1 LSB). */
+zt_status zt_image_to_rgb8_device(const double* d_pixels, uint64_t n_pixels, uint32_t tonemap, double gamma,
+                                  double exposure, uint8_t* d_rgb_out, void* stream);
+/* png.writePng (src/png.zig:10-58): the file size for a width x height RGB8
+ * image; ZT_ERR_INVALID_ARGUMENT with "InvalidDimensions" (0 or above
+ * 2^31-1) or "ImageTooLarge" (zlib stream above 2^31-1 bytes) as the
+ * reference reports. */
+zt_status zt_png_size(uint64_t width, uint64_t height, uint64_t* bytes_out);
+/* png.writePng into a caller buffer of at least zt_png_size bytes: 8-bit
+ * RGB, no filtering, stored DEFLATE blocks, on the host. */
+zt_status zt_png_encode(const uint8_t* rgb, uint64_t width, uint64_t height, uint8_t* out, uint64_t out_capacity);
+/* The same file assembled on the device (d_rgb and d_out device pointers),
+ * asynchronous on `stream`; byte-identical to zt_png_encode. */
+zt_status zt_png_encode_device(const uint8_t* d_rgb, uint64_t width, uint64_t height, uint8_t* d_out,
+                               uint64_t out_capacity, void* stream);
+/* render + Image.toRgb8 (the CLI's output path, src/main.zig:243-258) with
+ * both stages on the device; only the W*H*3 bytes of rgb_out are copied back.
+ * cfg may be NULL. */
+zt_status zt_render_rgb8(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg, uint32_t tonemap,
+                         double gamma, double exposure, uint8_t* rgb_out);
+/* render + Image.toRgb8 + png.writePng with every stage on the device; only
+ * the PNG file (zt_png_size bytes, png_capacity at least that) is copied
+ * back. */
+zt_status zt_render_png(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg, uint32_t tonemap,
+                        double gamma, double exposure, uint8_t* png_out, uint64_t png_capacity);
 
 const char* zt_last_error(void);
 /* Library version string. */

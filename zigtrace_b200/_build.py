@@ -28,9 +28,8 @@ NVCCFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xptxas", "-v", "
              "-fPIC,-ffp-contract=off,-fno-fast-math", f"-I{INCLUDE}", f"-I{CSRC}", *ARCH]
 
 CPP_SOURCES = ["scene_host.cpp"]
-CU_SOURCES = ["render.cu"]
-HEADERS = [CSRC / h for h in ("zt_types.h", "zt_device.cuh", "zt_fpmath.h", "scene_host.h")] + [
-    INCLUDE / "zigtrace_b200.h"]
+CU_SOURCES = ["render.cu", "output.cu", "bvh_build.cu"]
+HEADERS = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "zigtrace_b200.h"]
 
 
 def _newest(paths):

@@ -62,6 +62,7 @@ SIGNATURES = {
     "zt_scene_set_camera": (_i32, [_P, _P]),
     "zt_scene_set_background": (_i32, [_P, _P]),
     "zt_scene_build": (_i32, [_P]),
+    "zt_scene_build_device": (_i32, [_P, C.POINTER(_u32), C.POINTER(C.c_double)]),
     "zt_scene_counts": (_i32, [_P, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64),
                                C.POINTER(_u64)]),
     "zt_scene_bvh": (_i32, [_P, _P, _P]),
@@ -85,6 +86,12 @@ SIGNATURES = {
     "zt_trace_paths": (_i32, [_P, _P, _P, _P, _u64, _u64, _u32, _P]),
     "zt_rng_streams": (_i32, [_u64, _u64, _u64, _u64, _P]),
     "zt_image_to_rgb8": (_i32, [_P, _u64, _u32, C.c_double, C.c_double, _P]),
+    "zt_image_to_rgb8_device": (_i32, [_P, _u64, _u32, C.c_double, C.c_double, _P, _P]),
+    "zt_png_size": (_i32, [_u64, _u64, C.POINTER(_u64)]),
+    "zt_png_encode": (_i32, [_P, _u64, _u64, _P, _u64]),
+    "zt_png_encode_device": (_i32, [_P, _u64, _u64, _P, _u64, _P]),
+    "zt_render_rgb8": (_i32, [_P, _P, _P, _u32, C.c_double, C.c_double, _P]),
+    "zt_render_png": (_i32, [_P, _P, _P, _u32, C.c_double, C.c_double, _P, _u64]),
     "zt_last_error": (C.c_char_p, []),
     "zt_version": (C.c_char_p, []),
 }

@@ -254,7 +254,10 @@ class Scene:
         return self._n_shapes
 
     # -- build (scene.zig:90-96)
-    def build(self) -> "Scene":
+    def build(self, device: bool = False) -> "Scene":
+        """Scene.build.  device=True builds the BVH on the current CUDA
+        device (the same tree; see zt_scene_build_device); ``built_on_device``
+        and ``build_ms`` then report what happened."""
         lib = N.lib()
         self._invalidate()
         h = C.c_void_p()
@@ -268,7 +271,14 @@ class Scene:
             N.check(lib.zt_scene_add_shapes(h, N.ptr(shapes), len(shapes)))
         N.check(lib.zt_scene_set_camera(h, N.ptr(self.camera.record())))
         N.check(lib.zt_scene_set_background(h, N.ptr(self.background.record())))
-        N.check(lib.zt_scene_build(h))
+        self.built_on_device, self.build_ms = False, None
+        if device:
+            used, ms = C.c_uint32(), C.c_double()
+            N.check(lib.zt_scene_build_device(h, C.byref(used), C.byref(ms)))
+            self.built_on_device = bool(used.value)
+            self.build_ms = ms.value if used.value else None
+        else:
+            N.check(lib.zt_scene_build(h))
         return self
 
     @property
@@ -362,6 +372,43 @@ class Image:
         return rgb
 
 
+def png_size(width: int, height: int) -> int:
+    """Bytes of the PNG file png.writePng writes (src/png.zig:10-58)."""
+    n = C.c_uint64()
+    N.check(N.lib().zt_png_size(width, height, C.byref(n)))
+    return n.value
+
+
+def encode_png(rgb: np.ndarray, width: int, height: int) -> bytes:
+    """png.writePng (src/png.zig:10-58) on the host: 8-bit RGB, no filtering,
+    stored DEFLATE blocks."""
+    n = png_size(width, height)
+    src = np.ascontiguousarray(np.asarray(rgb, np.uint8).reshape(-1))
+    if src.size != width * height * 3:
+        raise ZigtraceError(-5, "rgb must hold width*height*3 bytes")
+    out = np.zeros(n, np.uint8)
+    N.check(N.lib().zt_png_encode(N.ptr(src), width, height, N.ptr(out), n))
+    return out.tobytes()
+
+
+def write_png(f, width: int, height: int, rgb: np.ndarray) -> None:
+    """png.writePng to a binary file object."""
+    f.write(encode_png(rgb, width, height))
+
+
+def image_to_rgb8_device(d_pixels: int, n_pixels: int, d_rgb_out: int, out: Output = Output(),
+                         stream: int = 0) -> None:
+    """Image.toRgb8 on the device between two device buffers (pointers as ints)."""
+    N.check(N.lib().zt_image_to_rgb8_device(C.c_void_p(d_pixels), n_pixels, TONEMAPS[out.tonemap], out.gamma,
+                                            out.exposure, C.c_void_p(d_rgb_out), C.c_void_p(stream)))
+
+
+def encode_png_device(d_rgb: int, width: int, height: int, d_out: int, capacity: int, stream: int = 0) -> None:
+    """png.writePng assembled on the device between two device buffers."""
+    N.check(N.lib().zt_png_encode_device(C.c_void_p(d_rgb), width, height, C.c_void_p(d_out), capacity,
+                                         C.c_void_p(stream)))
+
+
 def write_ppm(f, width: int, height: int, rgb: np.ndarray) -> None:
     """Binary P6 PPM, src/image.zig:77-81."""
     assert rgb.size == width * height * 3
@@ -377,6 +424,28 @@ def render(scene: Scene, opts: Options, gpu: Optional[GpuConfig] = None) -> Imag
     cfg = gpu.record() if gpu is not None else None
     N.check(N.lib().zt_render_ex(scene.handle, N.ptr(rec), N.ptr(cfg) if cfg is not None else None, N.ptr(out)))
     return Image(int(opts.width), int(opts.height), out.reshape(-1, 3))
+
+
+def render_rgb8(scene: Scene, opts: Options, out: Output = Output(), gpu: Optional[GpuConfig] = None) -> np.ndarray:
+    """render + Image.toRgb8 with both stages on the device (W*H*3 bytes)."""
+    rec = opts.record()
+    cfg = gpu.record() if gpu is not None else None
+    rgb = np.zeros(int(opts.width) * int(opts.height) * 3, np.uint8)
+    N.check(N.lib().zt_render_rgb8(scene.handle, N.ptr(rec), N.ptr(cfg) if cfg is not None else None,
+                                   TONEMAPS[out.tonemap], out.gamma, out.exposure, N.ptr(rgb)))
+    return rgb
+
+
+def render_png(scene: Scene, opts: Options, out: Output = Output(), gpu: Optional[GpuConfig] = None) -> bytes:
+    """render + Image.toRgb8 + png.writePng with every stage on the device:
+    the bytes of the PNG file."""
+    rec = opts.record()
+    cfg = gpu.record() if gpu is not None else None
+    n = png_size(int(opts.width), int(opts.height))
+    buf = np.zeros(n, np.uint8)
+    N.check(N.lib().zt_render_png(scene.handle, N.ptr(rec), N.ptr(cfg) if cfg is not None else None,
+                                  TONEMAPS[out.tonemap], out.gamma, out.exposure, N.ptr(buf), n))
+    return buf.tobytes()
 
 
 def render_device(scene: Scene, opts: Options, d_out_ptr: int, stream_ptr: int,

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "scene_host.h"
+#include "output.cuh"
 #include "wavefront.cuh"
 #include "zt_device.cuh"
 #include "zt_diff.cuh"
@@ -867,6 +868,55 @@ zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cf
 }
 
 zt_status zt_render(zt_scene* s, const zt_options* o, double* out) { return zt_render_ex(s, o, nullptr, out); }
+
+/* Render, encode and (for PNG) assemble the file on the device; only the
+ * encoded bytes cross PCIe.  One device allocation holds the framebuffer,
+ * the RGB8 image, the PNG and its checksum scratch. */
+static zt_status render_encoded(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, uint32_t tonemap,
+                                double gamma, double exposure, bool png, uint8_t* out, uint64_t capacity) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!out) return fail(ZT_ERR_INVALID_ARGUMENT, "NULL output");
+  if (tonemap > 2) return fail(ZT_ERR_INVALID_ARGUMENT, "tonemap must be 0 (none), 1 (reinhard) or 2 (aces)");
+  PngLayout L{};
+  const uint64_t npix = o->width * o->height;
+  uint64_t out_bytes = 3 * npix;
+  if (png) {
+    if ((rc = zt_png_size(o->width, o->height, &out_bytes)) != ZT_OK) return rc;
+    L = png_layout(o->width, o->height);
+  }
+  if (capacity < out_bytes) return fail(ZT_ERR_INVALID_ARGUMENT, "output buffer too small");
+  if ((rc = upload(s)) != ZT_OK) return rc;
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t fb_bytes = up(npix * 3 * sizeof(double)), rgb_bytes = up(npix * 3);
+  const size_t png_bytes = png ? up(L.total) : 0, scratch_bytes = png ? up(png_scratch_bytes(L)) : 0;
+  unsigned char* block = nullptr;
+  ZT_CUDA(cudaMalloc((void**)&block, fb_bytes + rgb_bytes + png_bytes + scratch_bytes), "allocate output buffers");
+  double* d_fb = reinterpret_cast<double*>(block);
+  uint8_t* d_rgb = block + fb_bytes;
+  uint8_t* d_png = d_rgb + rgb_bytes;
+  rc = launch_render(s, o, cfg, d_fb, 0);
+  if (rc == ZT_OK) rc = launch_encode_rgb8(d_fb, 3 * npix, tonemap, gamma, exposure, d_rgb, 0);
+  if (rc == ZT_OK && png) rc = launch_png(d_rgb, L, d_png, d_png + png_bytes, 0);
+  if (rc == ZT_OK) {
+    const cudaError_t e = cudaMemcpy(out, png ? d_png : d_rgb, out_bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(e, "copy encoded image");
+    else rc = wavefront_status(s, cfg);
+  }
+  cudaFree(block);
+  return rc;
+}
+
+zt_status zt_render_rgb8(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, uint32_t tonemap, double gamma,
+                         double exposure, uint8_t* rgb_out) {
+  if (!o) return fail(ZT_ERR_INVALID_ARGUMENT, "NULL options");
+  return render_encoded(s, o, cfg, tonemap, gamma, exposure, false, rgb_out, o->width * o->height * 3);
+}
+
+zt_status zt_render_png(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, uint32_t tonemap, double gamma,
+                        double exposure, uint8_t* png_out, uint64_t png_capacity) {
+  return render_encoded(s, o, cfg, tonemap, gamma, exposure, true, png_out, png_capacity);
+}
 
 zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end, double* out) {
   zt_status rc = check_render_args(s, o);

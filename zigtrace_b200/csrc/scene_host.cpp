@@ -261,7 +261,7 @@ static zt_status build_lights(zt_scene* s) {
   return ZT_OK;
 }
 
-zt_status build_scene(zt_scene* s) { /* Scene.build, scene.zig:92-96 */
+zt_status build_scene(zt_scene* s, bool device, bool* used_device, double* build_ms) { /* Scene.build, scene.zig:92-96 */
   for (const zt_shape& sh : s->shapes)
     if (sh.material >= s->materials.size()) return fail(ZT_ERR_INVALID_ARGUMENT, "shape refers to an undefined material");
   for (const zt_shape& sh : s->planes)
@@ -269,8 +269,14 @@ zt_status build_scene(zt_scene* s) { /* Scene.build, scene.zig:92-96 */
   release_staging(s);
   s->built = false;
   zt_status rc;
+  if (used_device) *used_device = false;
   try {
-    rc = build_bvh(s);
+    rc = ZT_DEVICE_BUILD_FALLBACK;
+    if (device) {
+      rc = device_build_bvh(s, build_ms);
+      if (rc == ZT_OK && used_device) *used_device = true;
+    }
+    if (rc == ZT_DEVICE_BUILD_FALLBACK) rc = build_bvh(s);
     if (rc == ZT_OK) rc = build_lights(s);
   } catch (const std::bad_alloc&) {
     return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory during Scene.build");
@@ -524,6 +530,14 @@ zt_status zt_scene_set_background(zt_scene* s, const zt_background* bg) {
 zt_status zt_scene_build(zt_scene* s) {
   if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_build: NULL scene");
   return build_scene(s);
+}
+
+zt_status zt_scene_build_device(zt_scene* s, uint32_t* used_device, double* build_ms) {
+  if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_build_device: NULL scene");
+  bool dev = false;
+  const zt_status rc = build_scene(s, true, &dev, build_ms);
+  if (used_device) *used_device = dev ? 1 : 0;
+  return rc;
 }
 
 zt_status zt_scene_counts(const zt_scene* s, uint64_t* nm, uint64_t* nb, uint64_t* np, uint64_t* nn, uint64_t* nl) {

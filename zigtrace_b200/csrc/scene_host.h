@@ -63,8 +63,16 @@ namespace zt {
 void set_error(const std::string& msg);
 zt_status fail(zt_status code, const std::string& msg);
 
-/* Scene.build (scene.zig:92-96). */
-zt_status build_scene(zt_scene* s);
+/* Scene.build (scene.zig:92-96); with device = true the BVH is built on the
+ * current CUDA device when it can be (see device_build_bvh), else on the
+ * host.  *used_device tells which. */
+zt_status build_scene(zt_scene* s, bool device = false, bool* used_device = nullptr, double* build_ms = nullptr);
+/* Bvh.build on the current CUDA device (bvh_build.cu): the same nodes and
+ * indices as the host build.  Returns ZT_DEVICE_BUILD_FALLBACK for input
+ * the device build leaves to the host (splitMedian nodes, non-finite
+ * boxes). */
+constexpr zt_status ZT_DEVICE_BUILD_FALLBACK = 1;
+zt_status device_build_bvh(zt_scene* s, double* build_ms);
 /* Camera.init (camera.zig:29-55) for the given aspect ratio. */
 DCamera camera_init(const zt_camera_config& cfg, double aspect);
 /* Flattens a built scene into the device layout. */

@@ -45,6 +45,10 @@ ZT_D double vlen(dv3 a) { return sqrt(vlen2(a)); }
 ZT_D dv3 vnorm(dv3 a) { return vdiv(a, vlen(a)); }
 ZT_D dv3 vlerp(dv3 a, dv3 b, double t) { return vscale(a, 1.0 - t) + vscale(b, t); }
 ZT_D double vmaxc(dv3 a) { return fmax(a.x, fmax(a.y, a.z)); }
+/* std.math.clamp(x, 0, 1) = @max(0, @min(x, 1)): a NaN x gives 1.  The NaN
+ * case is spelled out because nvcc may turn fmax(0, fmin(x, 1)) into a
+ * saturating operation, which maps NaN to 0 (measured on sm_100a). */
+ZT_D double clamp01(double x) { return isnan(x) ? 1.0 : fmax(0.0, fmin(x, 1.0)); }
 ZT_D bool vnear_zero(dv3 a) {
   const double eps = 1e-8;
   return fabs(a.x) < eps && fabs(a.y) < eps && fabs(a.z) < eps;
@@ -508,7 +512,7 @@ ZT_D void camera_ray(const DCamera& c, double s, double t, Rng& rng, dv3& ro, dv
 
 ZT_D dv3 background_radiance(const DBackground& bg, dv3 dir) { /* scene.zig:20-28 */
   if (bg.kind == 0) return L3(bg.a);
-  const double t = fmax(0.0, fmin(vnorm(dir).y, 1.0));
+  const double t = clamp01(vnorm(dir).y);
   return vlerp(L3(bg.a), L3(bg.b), t);
 }
 

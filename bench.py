@@ -206,7 +206,7 @@ def b200_arm(args):
         return diff_arm(args, world, rank, local_rank, barrier, allmax)
     scene, o = workload(args.workload, args.spp)
     o.seed = o.seed + rank  # each rank renders its own frame
-    scene.build()
+    scene.build(device=True)  # the same tree as the host build (zt_scene_build_device)
     counts = scene.counts()
     scene.upload()
     gcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity)
@@ -313,7 +313,9 @@ def b200_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
                    "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][args.mode],
-                   "sharding": "one frame per rank (seed = rank), no collective"},
+                   "sharding": "one frame per rank (seed = rank), no collective",
+                   "bvh_build": {"on_device": scene.built_on_device,
+                                 "device_ms": round(scene.build_ms, 2) if scene.build_ms else None}},
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
     }
     if rank == 0:

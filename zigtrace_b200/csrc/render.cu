@@ -566,9 +566,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(DevScene sc, RenderParams p, 
   const double* __restrict__ nee = w.nee;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t s = w.shadow_q[i];
-    double t;
-    const bool occluded = scene_query<true>(sc, ld3(nee, c, s, 0), ld3(nee, c, s, 3), kRayEpsilon,
-                                            nee[6 * (size_t)c + s], t) != -1;
+    const bool occluded = scene_occluded(sc, ld3(nee, c, s, 0), ld3(nee, c, s, 3), kRayEpsilon, nee[6 * (size_t)c + s]);
     const dv3 direct = occluded ? V(0, 0, 0) : ld3(nee, c, s, 7);
     const dv3 rad = ld3(w.rad, c, s, 0) + vmul(ld3(nee, c, s, 10), direct);
     st3(w.rad, c, s, 0, rad);

@@ -36,7 +36,7 @@ NOMINAL_SM_MHZ = 1965.0
 # (dram__bytes_read.sum + dram__bytes_write.sum, one 8-spp launch of the
 # workload, --clock-control none) and scaled by samples per launch: traffic
 # grows with the samples traced.  Workloads without a capture report null.
-NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 3.347888e9 / (1920 * 1080 * 8)}
+NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 2.527835e9 / (1920 * 1080 * 8)}
 
 
 def parse_args():

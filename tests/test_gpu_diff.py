@@ -2,9 +2,10 @@
 plain render at the scene's own colours, and with the oracle's detached
 forward at other colours), and the path-replay adjoint against central finite
 differences with common random numbers, on the device and on the CPU
-oracle.  Tolerance: the north star asks for gradients within 2% of FD; with
-detached sampling each sample is a polynomial in the colours, so the
-adjoint and FD agree far closer and the tests use 1e-4 relative."""
+oracle.  Tolerance: the target is gradients within 2% of finite
+differences; with detached sampling each sample is a polynomial in the
+colours, so the adjoint and FD agree far closer and the tests use 1e-4
+relative."""
 import numpy as np
 import pytest
 

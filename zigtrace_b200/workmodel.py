@@ -5,7 +5,7 @@ goes to f64 arithmetic in BVH traversal and shading, and to dependent loads
 of BVH records.  Work is counted per sample by the instrumented oracle on the
 same workload (counts of box tests, primitive tests, hits and light samples),
 then converted with fixed per-operation costs counted from the reference's
-arithmetic (f64 add/sub/mul/div/sqrt, no FMA in this build; compares not
+arithmetic (f64 add/sub/mul/div/sqrt, no FMA in the renderer; compares not
 counted):
 
   box slab test       12  (aabb.zig:74-75: 2 sub + 2 mul per axis)

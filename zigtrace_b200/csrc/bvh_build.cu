@@ -95,35 +95,49 @@ __device__ __forceinline__ uint32_t bin_of(double c, double lo, double extent) {
 
 struct Split { int axis; uint32_t bin; double cost; bool valid; };
 
-/* Builder.findSplit's sweeps (bvh.zig:211-256) over bins already reduced:
- * bin_box[axis][b], bin_n[axis][b]; axes with !(extent > 0) are skipped. */
+/* Builder.findSplit's sweeps (bvh.zig:211-256) for one axis, over its 12
+ * bins already reduced (bb[b] boxes, bn[b] counts): the best split of the
+ * axis, the first bin of the lowest cost. */
+template <typename BinBox>
+__device__ Split sweep_axis(const BinBox& bb, const uint32_t* bn, int axis, double parent_area) {
+  Split best{0, 0, 0.0, false};
+  double right_area[kBins];
+  uint32_t right_n[kBins];
+  DBox acc = dbox_empty();
+  uint32_t acc_n = 0;
+  for (int i = kBins - 1; i >= 0; --i) {
+    dbox_merge(acc, bb(i));
+    acc_n += bn[i];
+    right_area[i] = dbox_area(acc);
+    right_n[i] = acc_n;
+  }
+  acc = dbox_empty();
+  acc_n = 0;
+  for (int b = 0; b < kBins - 1; ++b) {
+    dbox_merge(acc, bb(b));
+    acc_n += bn[b];
+    const uint32_t rn = right_n[b + 1];
+    if (acc_n == 0 || rn == 0) continue;
+    const double cost = kTravCost + (dbox_area(acc) * (double)acc_n + right_area[b + 1] * (double)rn) / parent_area;
+    if (!best.valid || cost < best.cost) best = Split{axis, (uint32_t)b, cost, true};
+  }
+  return best;
+}
+
+/* The candidates of the three axes in axis order, as findSplit's single
+ * loop keeps them: a later axis wins only with a strictly lower cost. */
+__device__ __forceinline__ void keep_better(Split& best, const Split& c) {
+  if (c.valid && (!best.valid || c.cost < best.cost)) best = c;
+}
+
+/* findSplit over all three axes (one thread). */
 __device__ Split sweep(const DBox* bin_box, const uint32_t* bin_n, const bool* axis_ok, double parent_area) {
   Split best{0, 0, 0.0, false};
   if (parent_area <= 0) return best;
   for (int axis = 0; axis < 3; ++axis) {
     if (!axis_ok[axis]) continue;
     const DBox* bb = bin_box + axis * kBins;
-    const uint32_t* bn = bin_n + axis * kBins;
-    double right_area[kBins];
-    uint32_t right_n[kBins];
-    DBox acc = dbox_empty();
-    uint32_t acc_n = 0;
-    for (int i = kBins - 1; i >= 0; --i) {
-      dbox_merge(acc, bb[i]);
-      acc_n += bn[i];
-      right_area[i] = dbox_area(acc);
-      right_n[i] = acc_n;
-    }
-    acc = dbox_empty();
-    acc_n = 0;
-    for (int b = 0; b < kBins - 1; ++b) {
-      dbox_merge(acc, bb[b]);
-      acc_n += bn[b];
-      const uint32_t rn = right_n[b + 1];
-      if (acc_n == 0 || rn == 0) continue;
-      const double cost = kTravCost + (dbox_area(acc) * (double)acc_n + right_area[b + 1] * (double)rn) / parent_area;
-      if (!best.valid || cost < best.cost) best = Split{axis, (uint32_t)b, cost, true};
-    }
+    keep_better(best, sweep_axis([&](int b) { return bb[b]; }, bin_n + axis * kBins, axis, parent_area));
   }
   return best;
 }
@@ -523,7 +537,7 @@ struct LNode {       /* one node of a warp-built subtree, in visit (preorder) or
 
 constexpr int kWarpsPerBlock = 4;
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_small(Subtree* __restrict__ subs, uint32_t n_subs,
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 8) k_small(Subtree* __restrict__ subs, uint32_t n_subs,
                                                               uint32_t* __restrict__ idx,
                                                               const DBox* __restrict__ boxes,
                                                               const double* __restrict__ cent,
@@ -618,19 +632,31 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_small(Subtree* __restri
         }
       }
       __syncwarp();
-      if (lane == 0) {
-        DBox bin_box[3 * kBins];
-        for (int i = 0; i < 3 * kBins; ++i)
-          for (int k = 0; k < 3; ++k) {
-            bin_box[i].mn[k] = sbb[w][i][k];
-            bin_box[i].mx[k] = sbb[w][i][3 + k];
-          }
-        sp_best = sweep(bin_box, sbn[w], axis_ok, dbox_area(bounds));
+      /* one lane per axis runs findSplit's sweep; lane 0 keeps the best in
+       * axis order */
+      const double parent_area = dbox_area(bounds);
+      Split mine{0, 0, 0.0, false};
+      if (lane < 3 && parent_area > 0 && axis_ok[lane]) {
+        const int base = lane * kBins;
+        mine = sweep_axis(
+            [&](int b) {
+              DBox r;
+              for (int k = 0; k < 3; ++k) {
+                r.mn[k] = sbb[w][base + b][k];
+                r.mx[k] = sbb[w][base + b][3 + k];
+              }
+              return r;
+            },
+            sbn[w] + base, lane, parent_area);
       }
-      sp_best.valid = __shfl_sync(0xffffffffu, sp_best.valid, 0);
-      sp_best.axis = __shfl_sync(0xffffffffu, sp_best.axis, 0);
-      sp_best.bin = __shfl_sync(0xffffffffu, sp_best.bin, 0);
-      sp_best.cost = __shfl_sync(0xffffffffu, sp_best.cost, 0);
+      for (int a = 0; a < 3; ++a) {
+        Split c;
+        c.valid = __shfl_sync(0xffffffffu, mine.valid, a);
+        c.axis = __shfl_sync(0xffffffffu, mine.axis, a);
+        c.bin = __shfl_sync(0xffffffffu, mine.bin, a);
+        c.cost = __shfl_sync(0xffffffffu, mine.cost, a);
+        keep_better(sp_best, c);
+      }
       if (!sp_best.valid) {
         if (c > kLeafSize && lane == 0) atomicExch(fallback, 1); /* splitMedian: host */
         split = false;

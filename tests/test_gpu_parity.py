@@ -99,6 +99,15 @@ def test_triangle_heavy_subset_bit_exact(mode):
 
 
 @pytest.mark.parametrize("mode", MODES)
+def test_triangle_heavy_benchmark_config_subset_bit_exact(mode):
+    """The benchmark configuration itself (1920x1080, 64 spp, depth 16, BVH
+    built on the device); 150 oracle pixels."""
+    scene = scenes.triangle_heavy().build(device=True)
+    assert scene.built_on_device
+    _subset_check(scene, scenes.TRIANGLE_HEAVY_OPTIONS, 150, mode, seed=3)
+
+
+@pytest.mark.parametrize("mode", MODES)
 def test_render_is_deterministic_and_seed_dependent(mode):
     scene = scenes.random_spheres().build()
     o = zt.Options(320, 180, 4, 50, seed=7)

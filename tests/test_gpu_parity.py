@@ -146,6 +146,17 @@ def test_row_bands_reassemble_the_image():
         sharding.render_rows(scene, o, 50, 40)
 
 
+def test_row_bands_of_a_closed_scene_reassemble_the_image():
+    """Cornell box: AUTO and zt_render_rows take the regeneration kernel."""
+    from zigtrace_b200 import sharding
+    scene = scenes.cornell().build()
+    o = zt.Options(96, 71, 3, 16, seed=9)
+    full = zt.render(scene, o).pixels
+    assert full.tobytes() == O.OracleScene.from_scene(scene).render(96, 71, 3, 16, seed=9).tobytes()
+    parts = [sharding.render_rows(scene, o, a, b) for a, b in sharding.row_bands(o.height, 4)]
+    assert np.concatenate(parts).tobytes() == full.tobytes()
+
+
 def test_render_sharded_over_nccl_single_rank():
     import os
     import socket

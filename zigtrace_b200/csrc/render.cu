@@ -941,7 +941,7 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   }
   double* d_out = nullptr;
   ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
-  rc = launch_mega(s, p, 0, d_out, kMegaNested, 0);
+  rc = launch_mega(s, p, 0, d_out, s->device->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested, 0);
   if (rc == ZT_OK) {
     const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");

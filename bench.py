@@ -37,6 +37,10 @@ NOMINAL_SM_MHZ = 1965.0
 # workload, --clock-control none) and scaled by samples per launch: traffic
 # grows with the samples traced.  Workloads without a capture report null.
 NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 2.527835e9 / (1920 * 1080 * 8)}
+# What bounds the kernel instead of a pipe peak, from the same capture:
+# issue slots used, lanes active per warp instruction, FP64 pipe activity.
+NCU_EXECUTION = {"triangle_heavy": {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
+                                    "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3}}
 
 
 def parse_args():
@@ -296,6 +300,7 @@ def b200_arm(args):
             "traffic": (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
                         if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
             "traffic_note": "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
+            "ncu_execution": NCU_EXECUTION.get(args.workload) if args.mode in (0, 1) else None,
             "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
                            "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
             "algorithmic_flop_per_sample": round(work["flop"], 1),

@@ -176,6 +176,16 @@ zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu
 zt_status zt_forward(zt_scene* scene, const zt_options* opts, const double* colors, double* out_rgb);
 zt_status zt_backward(zt_scene* scene, const zt_options* opts, const double* colors, const double* d_image,
                       double* d_colors);
+/* The same for the image rows [row_begin, row_end) (one band of a frame
+ * sharded across GPUs): out_rgb and d_image hold the band's rows only,
+ * d_colors the band's share of the gradient (the shares of all bands sum to
+ * zt_backward's).  A zt_backward_rows after a zt_forward_rows over a band
+ * containing its rows, with the same options and colours, reuses the
+ * forward's primal radiance. */
+zt_status zt_forward_rows(zt_scene* scene, const zt_options* opts, uint64_t row_begin, uint64_t row_end,
+                          const double* colors, double* out_rgb);
+zt_status zt_backward_rows(zt_scene* scene, const zt_options* opts, uint64_t row_begin, uint64_t row_end,
+                           const double* colors, const double* d_image, double* d_colors);
 
 /* ---- Batched form: many renders in one persistent launch --------------- */
 /* n renders (scenes[i] with opts[i] into the device buffer d_outs[i] of

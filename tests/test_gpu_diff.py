@@ -105,3 +105,53 @@ def test_autograd_function_and_descent_reduce_the_loss():
             radiance.clamp_(min=0.0)
         losses.append(loss.item())
     assert losses[-1] < 0.3 * losses[0]
+
+
+def test_row_bands_of_forward_and_backward():
+    """zt_forward_rows bands concatenate to zt_forward's image bit for bit;
+    zt_backward_rows shares sum to zt_backward's gradient (atomics: the last
+    bits may differ), with and without the forward's primal cache."""
+    scene, target, _ = small()
+    o = zt.Options(64, 48, 4, 16)
+    rng = np.random.default_rng(5)
+    th = np.array([m["color"] for m in scene.materials]) * rng.uniform(0.9, 1.1, (len(scene.materials), 3))
+    full = zt.forward(scene, o, th).pixels
+    bands = [(0, 13), (13, 30), (30, 48)]
+    parts = [zt.forward_rows(scene, o, a, b, th) for a, b in bands]
+    assert np.concatenate(parts).tobytes() == full.tobytes()
+    d = 2.0 * (full - 0.25)
+    want = zt.backward(scene, o, d, th)
+    for warm in (True, False):
+        if warm:
+            zt.forward(scene, o, th)  # cache covers every band
+        else:
+            zt.forward_rows(scene, o, 0, 5, th)  # cache of another band: recomputed
+        got = sum(zt.backward_rows(scene, o, a, b, d[a * 64:b * 64], th) for a, b in bands)
+        assert np.allclose(got, want, rtol=1e-10, atol=1e-12)
+
+
+def test_sharded_forward_backward_over_nccl_single_rank():
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from zigtrace_b200 import sharding
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        scene, _, _ = small()
+        o = zt.Options(48, 32, 2, 16)
+        img = sharding.forward_sharded(scene, o)
+        assert img.tobytes() == zt.forward(scene, o).pixels.tobytes()
+        d = img - 0.1
+        g = sharding.backward_sharded(scene, o, d)
+        assert np.allclose(g, zt.backward(scene, o, d), rtol=1e-10, atol=1e-12)
+        items = scenes.batch_workload(count=6, seed=3)
+        imgs = sharding.render_batch_sharded([sc.build() for sc, _ in items], [op for _, op in items])
+        for (sc, op), im in zip(items, imgs):
+            assert im.tobytes() == zt.render(sc, op).pixels.tobytes()
+    finally:
+        dist.destroy_process_group()

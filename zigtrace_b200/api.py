@@ -535,6 +535,28 @@ def backward(scene: Scene, opts: Options, d_image, colors=None) -> np.ndarray:
     return out.reshape(-1, 3)
 
 
+def forward_rows(scene: Scene, opts: Options, y0: int, y1: int, colors=None) -> np.ndarray:
+    """Rows [y0, y1) of forward()'s image ((y1-y0)*width x 3), zt_forward_rows."""
+    c = _colors_arg(scene, colors)
+    out = np.zeros(max(y1 - y0, 0) * int(opts.width) * 3 + 1, np.float64)  # the C ABI validates the band
+    N.check(N.lib().zt_forward_rows(scene.handle, N.ptr(opts.record()), y0, y1, N.ptr(c) if c is not None else None,
+                                    N.ptr(out)))
+    return out[:-1].reshape(-1, 3)
+
+
+def backward_rows(scene: Scene, opts: Options, y0: int, y1: int, d_band, colors=None) -> np.ndarray:
+    """The share of dL/dcolors of image rows [y0, y1): d_band is dL/d(those
+    rows) ((y1-y0)*width x 3); the shares of all bands sum to backward()'s."""
+    c = _colors_arg(scene, colors)
+    g = np.ascontiguousarray(np.asarray(d_band, np.float64).reshape(-1))
+    if g.size != max(y1 - y0, 0) * int(opts.width) * 3:
+        raise ZigtraceError(-5, "d_band must hold (y1-y0)*width*3 values")
+    out = np.zeros(3 * len(scene.materials), np.float64)
+    N.check(N.lib().zt_backward_rows(scene.handle, N.ptr(opts.record()), y0, y1, N.ptr(c) if c is not None else None,
+                                     N.ptr(g if g.size else np.zeros(1)), N.ptr(out)))
+    return out.reshape(-1, 3)
+
+
 def set_colors(scene: Scene, colors) -> Scene:
     """Makes `colors` the scene's own material colours (they then also drive
     sampling) and rebuilds it."""

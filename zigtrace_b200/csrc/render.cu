@@ -58,6 +58,7 @@ struct zt_diff_cache {
   size_t cap = 0; /* doubles */
   bool valid = false;
   zt_options opts{};
+  uint64_t row0 = 0, rows = 0; /* the band the cached samples belong to */
   std::vector<double> theta;
 };
 
@@ -1067,15 +1068,16 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, Rend
                                                              const double* __restrict__ theta,
                                                              double* __restrict__ out, double* __restrict__ sample_L,
                                                              unsigned int* __restrict__ counter) {
-  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
+  const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
     unsigned tile = 0;
     if (lane == 0) tile = atomicAdd(counter, 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) return;
-    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
-    if (x >= p.width || y >= p.height) continue;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
+    if (x >= p.width || y >= row_end) continue;
     const uint64_t pix = y * p.width + x;
     Rng rng = rng_for_stream(p.seed, pix);
     dv3 sum = V(0, 0, 0);
@@ -1095,9 +1097,10 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, Rend
       if (visfinite(c)) sum = sum + c;
     }
     const dv3 px = vscale(sum, 1.0 / (double)p.spp);
-    out[3 * pix + 0] = px.x;
-    out[3 * pix + 1] = px.y;
-    out[3 * pix + 2] = px.z;
+    const uint64_t o = pix - p.row0 * p.width; /* output starts at the band's first row */
+    out[3 * o + 0] = px.x;
+    out[3 * o + 1] = px.y;
+    out[3 * o + 2] = px.z;
   }
 }
 
@@ -1118,7 +1121,8 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, Ren
     for (uint32_t i = threadIdx.x; i < n_params * (BS / 32); i += BS) sgrad[i] = 0.0;
     __syncthreads();
   }
-  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.height + 3) / 4);
+  const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
+  const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
   const double inv_spp = 1.0 / (double)p.spp;
   for (;;) {
@@ -1126,10 +1130,11 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, Ren
     if (lane == 0) tile = atomicAdd(counter, 1u);
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) break;
-    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = (tile / tiles_x) * 4 + (lane >> 3);
-    if (x >= p.width || y >= p.height) continue;
+    const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
+    if (x >= p.width || y >= row_end) continue;
     const uint64_t pix = y * p.width + x;
-    const dv3 adj = vscale(L3(dimg + 3 * pix), inv_spp); /* pixel = sum * (1/spp), render.zig:144 */
+    /* dL/dpixel of the band (rows row0 ..), pixel = sum * (1/spp), render.zig:144 */
+    const dv3 adj = vscale(L3(dimg + 3 * (pix - p.row0 * p.width)), inv_spp);
     if (adj.x == 0 && adj.y == 0 && adj.z == 0) continue;
     Rng rng = rng_for_stream(p.seed, pix);
     for (uint64_t i = 0; i < p.spp; ++i) {
@@ -1206,12 +1211,22 @@ static bool same_render(const zt_options& a, const zt_options& b) {
 extern "C" {
 
 zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, double* out) {
+  if (!o) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_forward: NULL options");
+  return zt_forward_rows(s, o, 0, o->height, colors, out);
+}
+
+zt_status zt_forward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end,
+                          const double* colors, double* out) {
   zt_status rc = check_render_args(s, o);
   if (rc != ZT_OK) return rc;
   if (!out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_forward: NULL output");
+  if (row_begin >= row_end || row_end > o->height)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_forward_rows: need row_begin < row_end <= height");
   if ((rc = upload(s)) != ZT_OK) return rc;
-  const RenderParams p = make_params(s, o);
-  const size_t bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  RenderParams p = make_params(s, o);
+  p.row0 = row_begin;
+  p.rows = row_end - row_begin;
+  const size_t bytes = (size_t)(p.rows * o->width * 3) * sizeof(double);
   zt_diff_cache& cache = s->device->diff;
   cache.valid = false;
   if (p.max_depth == 0) {
@@ -1222,7 +1237,8 @@ zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, dou
   double *d_theta = nullptr, *d_out = nullptr;
   if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
   /* keep every sample's primal radiance for a following zt_backward (24 bytes
-   * per sample); if that memory is not available the backward recomputes it */
+   * per sample, indexed by image pixel); if that memory is not available the
+   * backward recomputes it */
   const size_t n_l = (size_t)(p.width * p.height * p.spp) * 3;
   if (cache.cap < n_l) {
     cudaFree(cache.L);
@@ -1234,7 +1250,7 @@ zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, dou
   cudaError_t e = cudaMalloc((void**)&d_out, bytes);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
   if (e == cudaSuccess) {
-    k_forward_diff<128><<<persistent_grid(k_forward_diff<128>, 128, p.width * p.height), 128>>>(
+    k_forward_diff<128><<<persistent_grid(k_forward_diff<128>, 128, p.width * p.rows), 128>>>(
         launch_view(s), p, d_theta, d_out, cache.L, s->device->counter);
     e = cudaGetLastError();
   }
@@ -1245,6 +1261,8 @@ zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, dou
   if (cache.L) {
     cache.valid = true;
     cache.opts = *o;
+    cache.row0 = p.row0;
+    cache.rows = p.rows;
     cache.theta = th;
   }
   return ZT_OK;
@@ -1252,18 +1270,30 @@ zt_status zt_forward(zt_scene* s, const zt_options* o, const double* colors, dou
 
 zt_status zt_backward(zt_scene* s, const zt_options* o, const double* colors, const double* d_image,
                       double* d_colors) {
+  if (!o) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_backward: NULL options");
+  return zt_backward_rows(s, o, 0, o->height, colors, d_image, d_colors);
+}
+
+zt_status zt_backward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end,
+                           const double* colors, const double* d_image, double* d_colors) {
   zt_status rc = check_render_args(s, o);
   if (rc != ZT_OK) return rc;
   if (!d_image || !d_colors) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_backward: NULL argument");
+  if (row_begin >= row_end || row_end > o->height)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_backward_rows: need row_begin < row_end <= height");
   if ((rc = upload(s)) != ZT_OK) return rc;
-  const RenderParams p = make_params(s, o);
+  RenderParams p = make_params(s, o);
+  p.row0 = row_begin;
+  p.rows = row_end - row_begin;
   const uint32_t n_params = (uint32_t)(s->materials.size() * 3);
   memset(d_colors, 0, n_params * sizeof(double));
   if (p.max_depth == 0 || n_params == 0) return ZT_OK;
   const std::vector<double> th = theta_host(s, colors);
   const zt_diff_cache& cache = s->device->diff;
-  const double* sample_L = (cache.valid && same_render(cache.opts, *o) && cache.theta == th) ? cache.L : nullptr;
-  const size_t img_bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
+  const bool cached = cache.valid && same_render(cache.opts, *o) && cache.theta == th && cache.row0 <= p.row0 &&
+                      p.row0 + p.rows <= cache.row0 + cache.rows;
+  const double* sample_L = cached ? cache.L : nullptr;
+  const size_t img_bytes = (size_t)(p.rows * o->width * 3) * sizeof(double);
   double *d_theta = nullptr, *d_img = nullptr, *d_grad = nullptr;
   if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
   cudaError_t e = cudaMalloc((void**)&d_img, img_bytes);
@@ -1277,7 +1307,7 @@ zt_status zt_backward(zt_scene* s, const zt_options* o, const double* colors, co
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_backward_diff<128>, 128, use_smem ? smem : 0);
     uint64_t blocks = (uint64_t)sm_count() * (per_sm > 0 ? per_sm : 1);
-    const uint64_t need = (p.width * p.height + 127) / 128;
+    const uint64_t need = (p.width * p.rows + 127) / 128;
     if (blocks > need) blocks = need;
     k_backward_diff<128><<<(unsigned)blocks, 128, use_smem ? smem : 0>>>(
         launch_view(s), p, d_theta, d_img, d_grad, n_params, use_smem, sample_L, s->device->counter);

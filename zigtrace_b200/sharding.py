@@ -1,4 +1,4 @@
-"""One image across several GPUs, one process per GPU.
+"""Work split across GPUs, one process per GPU.
 
 Pixels are independent (each owns its RNG stream, src/render.zig:135), so
 rank r renders a contiguous band of image rows with zt_render_rows and the
@@ -6,6 +6,12 @@ bands are gathered with one all-gather over torch.distributed (NCCL on GPUs,
 gloo on CPU).  The gathered image is bit-identical to a one-device render.
 Bands can be balanced by a per-row cost estimate (e.g. the previous frame's
 per-row times); without one they split the rows evenly.
+
+The differentiable form splits the same way: each rank runs the forward and
+the path-replay backward of its band (zt_forward_rows / zt_backward_rows)
+and one all-reduce sums the gradient shares (3 values per material).  A
+batch of renders is split by estimated cost, longest first onto the least
+loaded rank (LPT), and the images are gathered on every rank.
 """
 from __future__ import annotations
 
@@ -15,7 +21,7 @@ from typing import Callable, List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _native as N
-from .api import Options, Scene
+from .api import Options, Scene, backward_rows, forward_rows, render
 
 
 def row_bands(height: int, world: int, row_costs: Optional[Sequence[float]] = None) -> List[Tuple[int, int]]:
@@ -73,3 +79,81 @@ def render_sharded(scene: Scene, opts: Options, group=None,
         n = (b - a) * width
         img[a * width:b * width] = part[:n * 3].cpu().numpy().reshape(-1, 3)
     return img
+
+
+def forward_sharded(scene: Scene, opts: Options, colors=None, group=None, row_costs=None,
+                    forward_band: Optional[Callable] = None) -> np.ndarray:
+    """forward() across the ranks of `group`: each rank's band by
+    zt_forward_rows, gathered as render_sharded does."""
+    band = forward_band or (lambda sc, o, y0, y1: forward_rows(sc, o, y0, y1, colors))
+    return render_sharded(scene, opts, group, render_band=band, row_costs=row_costs)
+
+
+def backward_sharded(scene: Scene, opts: Options, d_image, colors=None, group=None, row_costs=None,
+                     backward_band: Optional[Callable] = None) -> np.ndarray:
+    """backward() across the ranks of `group`: each rank computes the
+    gradient share of its band of rows, then one all-reduce sums the shares
+    (n_materials x 3 on every rank)."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    width = int(opts.width)
+    y0, y1 = row_bands(int(opts.height), world, row_costs)[rank]
+    g = np.asarray(d_image, np.float64).reshape(-1, 3)
+    band = backward_band or (lambda sc, o, a, b, d: backward_rows(sc, o, a, b, d, colors))
+    n = 3 * len(scene.materials)
+    share = band(scene, opts, y0, y1, g[y0 * width:y1 * width]) if y1 > y0 else np.zeros(n)
+    device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    t = torch.from_numpy(np.ascontiguousarray(share, np.float64).reshape(-1).copy()).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy().reshape(-1, 3)
+
+
+def assign_batch(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Longest-processing-time assignment: renders in decreasing cost (ties by
+    index) each go to the rank with the least assigned cost so far (ties to
+    the lower rank).  Returns the indices each rank renders, in input order."""
+    if world < 1:
+        raise ValueError("world must be positive")
+    c = np.asarray(costs, np.float64)
+    load = [0.0] * world
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(c)), key=lambda k: (-c[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += float(c[i])
+    return [sorted(p) for p in parts]
+
+
+def batch_costs(scenes: Sequence[Scene], opts_list: Sequence[Options]) -> List[float]:
+    """Cost estimate of each render: samples x log2(primitives + 2)."""
+    out = []
+    for sc, o in zip(scenes, opts_list):
+        n = sc.counts()["bounded"] + sc.counts()["planes"]
+        out.append(float(o.width * o.height * o.spp) * float(np.log2(n + 2)))
+    return out
+
+
+def render_batch_sharded(scenes: Sequence[Scene], opts_list: Sequence[Options], group=None,
+                         costs: Optional[Sequence[float]] = None,
+                         render_item: Optional[Callable] = None) -> List[np.ndarray]:
+    """Renders a batch across the ranks of `group` (LPT by cost) and returns
+    every image (height*width x 3), in input order, on every rank."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    costs = batch_costs(scenes, opts_list) if costs is None else costs
+    mine = assign_batch(costs, world)[rank]
+    fn = render_item or (lambda sc, o: render(sc, o).pixels)
+    local = {i: np.ascontiguousarray(fn(scenes[i], opts_list[i])) for i in mine}
+    gathered: list = [None] * world
+    dist.all_gather_object(gathered, local, group=group)
+    images: List[Optional[np.ndarray]] = [None] * len(scenes)
+    for part in gathered:
+        for i, img in part.items():
+            images[i] = img
+    return images  # type: ignore[return-value]

@@ -483,7 +483,7 @@ def diff_arm(args, world, rank, local_rank, barrier, allmax):
         torch.cuda.synchronize()
         barrier()
         ts = []
-        for _ in range(max(args.steps, 5)):  # host-timed calls: the median of at least 5 resists host jitter
+        for _ in range(max(args.steps, 9)):  # host-timed calls: the median of at least 9 resists host jitter
             t0 = time.perf_counter()
             fn()
             torch.cuda.synchronize()

@@ -119,7 +119,8 @@ zt_status zt_scene_build(zt_scene* scene);
  * primitive order and numbering as zt_scene_build (bvh.zig:41-262), node
  * bounds equal up to the sign of zero.  Scenes that need the reference's
  * median split (more than 4 primitives whose centroids coincide, or bounds
- * without area) or hold non-finite coordinates are built on the host;
+ * without area) or hold non-finite coordinates are built on the host, as are
+ * all scenes when no CUDA device (or too little device memory) is available;
  * *used_device (may be NULL) is 1 when the device built the BVH.
  * *build_ms (may be NULL) is the device time of the build. */
 zt_status zt_scene_build_device(zt_scene* scene, uint32_t* used_device, double* build_ms);

@@ -88,3 +88,15 @@ def test_write_ppm(native_lib):  # image.zig:114-126
     buf = io.BytesIO()
     zt.write_ppm(buf, 2, 1, img.to_rgb8())
     assert buf.getvalue() == b"P6\n2 1\n255\n\xff\x00\x00\x00\x00\xff"
+
+
+def test_device_build_falls_back_to_the_host_tree_without_a_gpu(native_lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present: the device build is checked by the gpu tests")
+    import kat_scenes as K
+    dev = K.random_shapes(3, 500).build(device=True)
+    host = K.random_shapes(3, 500).build()
+    assert not dev.built_on_device
+    (dn, di), (hn, hi) = dev.bvh(), host.bvh()
+    assert dn.tobytes() == hn.tobytes() and di.tobytes() == hi.tobytes()

@@ -35,7 +35,8 @@
  * Nodes that need splitMedian (more than 4 primitives and no bin split:
  * all centroids coincide or the bounds have no area) and boxes with
  * non-finite coordinates are left to the host builder: the build reports
- * ZT_DEVICE_BUILD_FALLBACK and the caller runs the host build instead.
+ * ZT_DEVICE_BUILD_FALLBACK and the caller runs the host build instead, as it
+ * does when no CUDA device or too little device memory is available.
  * Bounds agree with the host build up to the sign of zero (min and max of
  * +0 and -0 may return either); nothing downstream distinguishes the two.
  */
@@ -808,11 +809,11 @@ zt_status device_build_bvh(zt_scene* s, double* build_ms) {
   const size_t o_out = off; off += up((2 * n - 1) * sizeof(HostNode));
   unsigned char* mem = nullptr;
   cudaError_t e = cudaMalloc((void**)&mem, off);
-  if (e != cudaSuccess) {
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
+  if (e != cudaSuccess) { /* no device, or not enough device memory: the host builds it */
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
     cudaGetLastError();
-    return fail(ZT_ERR_OUT_OF_MEMORY, "device BVH build: cudaMalloc");
+    return ZT_DEVICE_BUILD_FALLBACK;
   }
   zt_shape* d_shapes = (zt_shape*)(mem + o_shapes);
   DBox* d_boxes = (DBox*)(mem + o_boxes);

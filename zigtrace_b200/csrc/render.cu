@@ -69,7 +69,6 @@ struct zt_device_buffers {
   DevScene view;
   zt_wavefront_cache wf;
   zt_diff_cache diff;
-  double mean_path = 0; /* mean path length of the upload-time pilot (AUTO's choice) */
 };
 
 namespace zt {
@@ -168,7 +167,7 @@ static zt_status upload(zt_scene* s) {
   if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
   int dev = 0;
   ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
-  if (s->device && s->device->device == dev) return ZT_OK;
+  if (s->device && s->device->device == dev) return s->pilot_valid ? ZT_OK : pilot_paths(s);
   release_device(s);
   zt_status rc = make_staging(s);
   if (rc != ZT_OK) return rc;
@@ -193,7 +192,7 @@ static zt_status upload(zt_scene* s) {
   d->view.mats = (const DMat*)(b + h->off_mats);
   d->view.lights = (const DLight*)(b + h->off_lights);
   d->view.cdf = (const double*)(b + h->off_cdf);
-  return pilot_paths(s);
+  return s->pilot_valid ? ZT_OK : pilot_paths(s);
 }
 
 /* The resident view with the scene's current background (the background can
@@ -363,9 +362,12 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
   }
 }
 
-/* The megakernel's tile loop over render_pixel_regen. */
+/* The megakernel's tile loop over render_pixel_regen.  Four blocks of 128
+ * per SM (up to 128 registers, no spills): 1.17x the seven-block build on the
+ * Cornell box, whose 65,536 pixels fill only a quarter of the GPU's thread
+ * slots anyway, and equal to it on 1280x720 random spheres. */
 template <int BS>
-__global__ void __launch_bounds__(BS, 896 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
+__global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
                                                              unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
@@ -796,7 +798,7 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
-  const bool long_paths = s->device->mean_path >= kRegenMeanPath;
+  const bool long_paths = s->pilot_valid && s->mean_path >= kRegenMeanPath;
   const MegaVariant variant =
       (mode == ZT_MODE_MEGAKERNEL_REGEN || (mode == ZT_MODE_AUTO && long_paths)) ? kMegaRegen : kMegaNested;
   return launch_mega(s, p, bs, d_out, variant, stream);
@@ -942,7 +944,7 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   }
   double* d_out = nullptr;
   ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
-  rc = launch_mega(s, p, 0, d_out, s->device->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested, 0);
+  rc = launch_mega(s, p, 0, d_out, s->pilot_valid && s->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested, 0);
   if (rc == ZT_OK) {
     const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");
@@ -951,7 +953,8 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   return rc;
 }
 
-/* Upload-time pilot for ZT_MODE_AUTO: the mean path length of one sample
+/* Pilot for ZT_MODE_AUTO, run by the synchronous entry points (upload)
+ * once per build, camera and background: the mean path length of one sample
  * per pixel of a 64x64 image from the scene's camera (depth 16).  Long paths
  * (closed scenes) favour the path-regeneration megakernel: on the Cornell box
  * (mean 3.4) it is 1.5x the nested one, on open scenes (random spheres 2.5,
@@ -982,7 +985,8 @@ static zt_status pilot_paths(zt_scene* s) {
   if (e != cudaSuccess) return cuda_fail(e, "pilot render");
   double sum = 0;
   for (uint32_t v : pl) sum += v;
-  s->device->mean_path = sum / (double)npix;
+  s->mean_path = sum / (double)npix;
+  s->pilot_valid = true;
   return ZT_OK;
 }
 }  // namespace zt

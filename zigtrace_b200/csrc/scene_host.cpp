@@ -268,6 +268,7 @@ zt_status build_scene(zt_scene* s, bool device, bool* used_device, double* build
     if (sh.material >= s->materials.size()) return fail(ZT_ERR_INVALID_ARGUMENT, "plane refers to an undefined material");
   release_staging(s);
   s->built = false;
+  s->pilot_valid = false;
   zt_status rc;
   if (used_device) *used_device = false;
   try {
@@ -516,6 +517,7 @@ zt_status zt_scene_add_quad(zt_scene* s, const zt_vec3* c, const zt_vec3* u, con
 
 zt_status zt_scene_set_camera(zt_scene* s, const zt_camera_config* cfg) {
   if (!s || !cfg) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_set_camera: NULL argument");
+  if (memcmp(&s->camera, cfg, sizeof *cfg) != 0) s->pilot_valid = false;
   s->camera = *cfg;
   return ZT_OK;
 }
@@ -523,6 +525,7 @@ zt_status zt_scene_set_camera(zt_scene* s, const zt_camera_config* cfg) {
 zt_status zt_scene_set_background(zt_scene* s, const zt_background* bg) {
   if (!s || !bg) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_set_background: NULL argument");
   if (bg->kind > ZT_BG_SKY) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown background kind");
+  if (memcmp(&s->background, bg, sizeof *bg) != 0) s->pilot_valid = false;
   s->background = *bg;
   return ZT_OK;
 }

@@ -55,6 +55,8 @@ struct zt_scene {
   std::vector<double> cdf;
   double total = 0;
   zt_device_buffers* device = nullptr;  /* resident copy, owned */
+  bool pilot_valid = false;             /* mean_path is current for this build, camera and background */
+  double mean_path = 0;                 /* mean path length of the pilot that ZT_MODE_AUTO reads */
   zt_host_staging* staging = nullptr;   /* pinned flattened copy, owned */
 };
 

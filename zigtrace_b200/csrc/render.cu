@@ -1066,9 +1066,13 @@ zt_status zt_rng_streams(uint64_t seed, uint64_t stream0, uint64_t n_streams, ui
 namespace zt {
 
 /* Forward of the detached estimator (zt_diff.cuh): the megakernel's tile
- * loop with trace_diff; theta == the scene's colours gives zt_render's image. */
+ * loop with trace_diff; theta == the scene's colours gives zt_render's image.
+ * The differentiable kernels are built for four blocks of 128 per SM (128
+ * registers): their longer code spills heavily at 72 registers, and at
+ * 512x512 the fewer resident warps measured faster (forward 28 vs 31 ms,
+ * backward 52 vs 57-62 ms). */
 template <int BS>
-__global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, RenderParams p,
+__global__ void __launch_bounds__(BS, 512 / BS) k_forward_diff(DevScene sc, RenderParams p,
                                                              const double* __restrict__ theta,
                                                              double* __restrict__ out, double* __restrict__ sample_L,
                                                              unsigned int* __restrict__ counter) {
@@ -1113,7 +1117,7 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_forward_diff(DevScene sc, Rend
  * dL/dtheta into per-block shared memory (flushed once per block), or
  * straight into global memory when the parameter table is large. */
 template <int BS>
-__global__ void __launch_bounds__(BS, 896 / BS) k_backward_diff(DevScene sc, RenderParams p,
+__global__ void __launch_bounds__(BS, 512 / BS) k_backward_diff(DevScene sc, RenderParams p,
                                                               const double* __restrict__ theta,
                                                               const double* __restrict__ dimg, double* grad,
                                                               uint32_t n_params, int use_smem,

@@ -173,3 +173,32 @@ def golden_cases() -> dict:
         "cornell_32x32_8spp": (scenes.cornell(), dict(width=32, height=32, spp=8, max_depth=16)),
         "spheres_64x36_2spp": (scenes.random_spheres(), dict(width=64, height=36, spp=2, max_depth=50)),
     }
+
+
+def fuzz_scene(seed: int) -> Scene:
+    """A random scene exercising every shape, material and light kind:
+    spheres (some with negative radius), triangles, quads, a plane, all four
+    materials (metal with and without fuzz, glass), emissive spheres and
+    quads as lights, a sky or a solid background, and a thin-lens camera."""
+    rng = np.random.default_rng(10_000 + seed)
+    s = Scene()
+    mats = [s.add_material(Material.lambertian(rng.uniform(0.1, 0.9, 3))),
+            s.add_material(Material.metal(rng.uniform(0.3, 1.0, 3), float(rng.choice([0.0, rng.uniform(0, 1)])))),
+            s.add_material(Material.dielectric(float(rng.uniform(1.2, 2.0)))),
+            s.add_material(Material.emissive(rng.uniform(1, 12, 3))),
+            s.add_material(Material.lambertian(rng.uniform(0.1, 0.9, 3)))]
+    s.add(plane((0, float(rng.uniform(-1.5, -0.5)), 0), (0, 1, 0), mats[4]))
+    for _ in range(int(rng.integers(4, 12))):
+        c = rng.uniform([-3, -1, -5], [3, 2, -1])
+        r = float(rng.uniform(0.2, 0.8)) * (-1 if rng.random() < 0.15 else 1)
+        s.add(sphere(c, r, int(rng.choice(mats))))
+    for _ in range(int(rng.integers(2, 8))):
+        c = rng.uniform([-3, -1, -5], [3, 2, -1])
+        s.add(triangle(c, c + rng.uniform(-1, 1, 3), c + rng.uniform(-1, 1, 3), int(rng.choice(mats[:3]))))
+    s.add_quad(rng.uniform([-1, 2.5, -3], [0, 3, -2]), (1.0, 0, 0), (0, 0, 1.0), mats[3])
+    s.add(sphere(rng.uniform([-2, 2, -4], [2, 3, -2]), float(rng.uniform(0.1, 0.4)), mats[3]))
+    s.background = Background.sky((1, 1, 1), (0.5, 0.7, 1.0)) if rng.random() < 0.5 else \
+        Background.solid(rng.uniform(0, 0.2, 3))
+    s.camera = CameraConfig(look_from=(float(rng.uniform(-1, 1)), 0.5, 3), look_at=(0, 0.2, -3), vfov=50,
+                            aperture=float(rng.choice([0.0, 0.1])), focus_dist=5.0)
+    return s

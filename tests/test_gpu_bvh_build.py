@@ -37,6 +37,8 @@ CASES = {
     "spheres": scenes.random_spheres,                            # ~320 spheres: large levels + warp subtrees
     "random_shapes_2000": lambda: K.random_shapes(3, 2000),
     "sphere_field_20000": lambda: scenes.sphere_field(5, 20000),
+    "fuzz_0": lambda: K.fuzz_scene(0),
+    "fuzz_1": lambda: K.fuzz_scene(1),
 }
 
 

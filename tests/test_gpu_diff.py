@@ -155,3 +155,11 @@ def test_sharded_forward_backward_over_nccl_single_rank():
             assert im.tobytes() == zt.render(sc, op).pixels.tobytes()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_forward_at_own_colors_on_fuzz_scenes(seed):
+    import kat_scenes as K
+    scene = K.fuzz_scene(seed).build()
+    o = zt.Options(32, 20, 3, 12, seed=seed)
+    assert zt.forward(scene, o).pixels.tobytes() == zt.render(scene, o).pixels.tobytes()

@@ -191,3 +191,15 @@ def test_edge_options(mode):
     with pytest.raises(zt.ZigtraceError) as ei:
         zt.render(scene, zt.Options(0, 4, 1, 1))
     assert ei.value.name == "InvalidOptions"
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("seed", range(8))
+def test_fuzz_scenes_bit_exact(seed, mode):
+    """Random scenes with every shape, material and light kind, lens
+    sampling and both backgrounds: whole image against the oracle."""
+    scene = K.fuzz_scene(seed).build()
+    o = zt.Options(32, 20, 3, 12, seed=seed)
+    img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
+    want = O.OracleScene.from_scene(scene).render(32, 20, 3, 12, seed=seed)
+    assert img.tobytes() == want.tobytes()

@@ -40,7 +40,37 @@ NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 2.527835e9 / (1920 * 1080 * 8)}
 # What bounds the kernel instead of a pipe peak, from the same capture:
 # issue slots used, lanes active per warp instruction, FP64 pipe activity.
 NCU_EXECUTION = {"triangle_heavy": {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
-                                    "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3}}
+                                    "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
+                 "batch": {"issue_active_pct": 60.5, "lanes_per_warp_instruction": 14.23,
+                           "fp64_pipe_active_pct": 37.5, "l1_hit_pct": 71.9, "l2_hit_pct": 87.1}}
+# The batched launch, captured whole (rank 0's batch, one launch).
+NCU_DRAM_BYTES_BATCH = 0.661207e9 + 6.302831e9
+
+
+def roofline_entry(work: dict, samples: int, kernel_ms: float, sms: int, traffic, traffic_note: str,
+                   execution) -> dict:
+    """The roofline object for one kernel: oracle-counted FLOP and bytes per
+    sample times the samples of one launch, over its CUDA-event duration."""
+    flop = work["flop"] * samples
+    achieved = flop / (kernel_ms / 1e3) / 1e12
+    peak = sms * FP64_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bytes_per_launch = work["bytes"] * samples
+    return {
+        "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": traffic, "traffic_note": traffic_note, "ncu_execution": execution,
+        "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
+                       "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
+        "algorithmic_flop_per_sample": round(work["flop"], 1),
+        "algorithmic_bytes_per_sample": round(work["bytes"], 1),
+        "kernel_ms": round(kernel_ms, 3),
+        "memory": {"achieved_gbs": round(bytes_per_launch / (kernel_ms / 1e3) / 1e9, 1), "peak_gbs": hbm,
+                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
+                   "note": "bytes requested from the memory system; most are served by L2"},
+        "per_sample": {k: round(v, 3) for k, v in work.items() if k not in ("flop", "bytes")},
+    }
 
 
 def parse_args():
@@ -288,29 +318,12 @@ def b200_arm(args):
     roofline = None
     if work is not None:
         sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-        flop = work["flop"] * samples
-        achieved = flop / (kernel_ms / 1e3) / 1e12
-        peak = sms * FP64_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-        hbm = peaks.get("hbm_gbs", 6650.0)
-        bytes_per_launch = work["bytes"] * samples
-        roofline = {
-            "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
-            "frac": round(achieved / peak, 4),
-            "traffic": (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
-                        if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
-            "traffic_note": "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
-            "ncu_execution": NCU_EXECUTION.get(args.workload) if args.mode in (0, 1) else None,
-            "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
-                           "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
-            "algorithmic_flop_per_sample": round(work["flop"], 1),
-            "algorithmic_bytes_per_sample": round(work["bytes"], 1),
-            "kernel_ms": round(kernel_ms, 3),
-            "memory": {"achieved_gbs": round(bytes_per_launch / (kernel_ms / 1e3) / 1e9, 1), "peak_gbs": hbm,
-                       "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
-                       "note": "bytes requested from the memory system; most are served by L2"},
-            "per_sample": {k: round(v, 3) for k, v in work.items() if k not in ("flop", "bytes")},
-        }
+        roofline = roofline_entry(
+            work, samples, kernel_ms, sms,
+            (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
+             if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
+            "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
+            NCU_EXECUTION.get(args.workload) if args.mode in (0, 1) else None)
 
     line = {
         "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world,
@@ -412,21 +425,37 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
         e2e["batched_over_plain_calls"] = round(plain_e2e_s / e2e_s, 3)
 
     cpu = None
+    roofline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle as O
+        from zigtrace_b200 import workmodel
         rng = np.random.default_rng(3)
         threads = os.cpu_count() or 1
         n_s, t_s = 0, 0.0
+        work_w = {}  # per-sample work of each sampled render, weighted by the render's samples
+        weight = 0
         for k in rng.choice(len(items), 32, replace=False):
             s, o = items[int(k)]
             os_ = O.OracleScene.from_scene(s)  # BVH build outside the timed region, as in the reference CLI
             pix = np.sort(rng.choice(o.width * o.height, min(1024, o.width * o.height), replace=False))
             t0 = time.perf_counter()
-            os_.render_pixels(o.width, o.height, o.spp, o.max_depth, pix.astype(np.uint64), threads=threads)
+            _, st = os_.render_pixels(o.width, o.height, o.spp, o.max_depth, pix.astype(np.uint64), threads=threads,
+                                      stats=True)
             t_s += time.perf_counter() - t0
             n_s += len(pix) * o.spp
+            w = o.width * o.height * o.spp
+            for key, v in workmodel.per_sample(st, o.spp).items():
+                work_w[key] = work_w.get(key, 0.0) + v * w
+            weight += w
         cpu = {"value": round(n_s / t_s / 1e6, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",
                "sample": f"1024 random pixels x 16 spp from each of 32 random renders of the batch ({n_s} samples)"}
+        sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        roofline = roofline_entry(
+            {key: v / weight for key, v in work_w.items()}, samples, batch_ms, sms, round(NCU_DRAM_BYTES_BATCH),
+            "DRAM bytes of one batched launch of this batch (seed 0), from an ncu capture",
+            NCU_EXECUTION["batch"])
+        roofline["work_note"] = ("per-sample work averaged over 32 sampled renders, each weighted by its samples "
+                                 "per step")
 
     line = {
         "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -442,7 +471,7 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
         "plain_launches": {"value": round(plain_value, 4), "unit": "Msamples/s", "ms_per_step": round(plain_ms, 3),
                            "launches_per_step": len(items)},
         "batched_over_plain": round(plain_ms / batch_ms, 3), "identical_images": bool(same),
-        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": None, "cpu_baseline": cpu,
+        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -227,8 +227,9 @@ static RenderParams make_params(const zt_scene* s, const zt_options* o) {
 
 /* ------------------------------------------------------------ Kernels ---- */
 
-/* One pixel: renderTile's per-pixel body, render.zig:133-144. */
-template <bool kAux>
+/* One pixel: renderTile's per-pixel body, render.zig:133-144.  kNee as for
+ * trace_with. */
+template <bool kAux, bool kNee = true>
 __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderParams& p, uint64_t pix,
                                              double* __restrict__ out, TraceAux* aux) {
   const uint64_t x = pix % p.width, y = pix / p.width;
@@ -241,7 +242,7 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
     const double t = ((double)y + rng_float(rng)) / h;
     dv3 ro, rd;
     camera_ray(p.cam, s, t, rng, ro, rd);
-    const dv3 c = trace_with<kAux>(sc, ro, rd, rng, p.max_depth, p.use_nee != 0, aux);
+    const dv3 c = trace_with<kAux, kNee>(sc, ro, rd, rng, p.max_depth, p.use_nee != 0, aux);
     if (kAux) break;
     if (visfinite(c)) sum = sum + c;
   }
@@ -258,10 +259,15 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
  * work counter until the image is exhausted (the device form of
  * Context.work's atomic tile counter, render.zig:113-119), so its camera rays
  * are coherent.  896 resident threads per SM (7 blocks of 128, <= 73
- * registers) measured fastest on the 1M-triangle workload among 512..1024. */
-template <int BS>
-__global__ void __launch_bounds__(BS, 896 / BS) k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out,
-                                                            unsigned int* __restrict__ counter) {
+ * registers) measured fastest on the 1M-triangle workload among 512..1024.
+ * The instance without light sampling (kNee = false) is a separate build
+ * with its own residency. */
+constexpr int kMegaThreadsPerSm = 896;
+constexpr int kMegaThreadsPerSmNoNee = 896;
+
+template <int BS, bool kNee>
+__global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
+    k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out, unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
@@ -271,7 +277,7 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_render_mega(DevScene sc, Rende
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) return;
     const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
-    if (x < p.width && y < row_end) render_pixel<false>(sc, p, y * p.width + x, out, nullptr);
+    if (x < p.width && y < row_end) render_pixel<false, kNee>(sc, p, y * p.width + x, out, nullptr);
   }
 }
 
@@ -396,10 +402,12 @@ struct BatchItem {
  * Warps take 8x4 tiles from one counter over the concatenated tile ranges of
  * all items (in the order the host chose, largest first by default) and
  * render them with the item's own scene and parameters, so small images do
- * not leave the GPU idle the way one launch per image does. */
-template <int BS>
-__global__ void __launch_bounds__(BS, 896 / BS) k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items,
-                                                             uint64_t total_tiles, unsigned int* __restrict__ counter) {
+ * not leave the GPU idle the way one launch per image does.  kNee = false
+ * is the instance for batches in which no render samples lights. */
+template <int BS, bool kNee>
+__global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
+    k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
+                   unsigned int* __restrict__ counter) {
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
     unsigned tile = 0;
@@ -415,7 +423,8 @@ __global__ void __launch_bounds__(BS, 896 / BS) k_render_batch(const BatchItem* 
     const BatchItem& it = items[lo];
     const uint64_t local = tile - it.tile_begin;
     const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
-    if (x < it.p.width && y < it.p.height) render_pixel<false>(it.sc, it.p, y * it.p.width + x, it.out, nullptr);
+    if (x < it.p.width && y < it.p.height)
+      render_pixel<false, kNee>(it.sc, it.p, y * it.p.width + x, it.out, nullptr);
   }
 }
 
@@ -654,8 +663,12 @@ static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_o
   const uint64_t npix = p.width * p.rows;
   if (variant == kMegaRegen)
     k_render_regen<BS><<<persistent_grid(k_render_regen<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
+  else if (p.use_nee)
+    k_render_mega<BS, true><<<persistent_grid(k_render_mega<BS, true>, BS, npix), BS, 0, stream>>>(v, p, d_out,
+                                                                                                    counter);
   else
-    k_render_mega<BS><<<persistent_grid(k_render_mega<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
+    k_render_mega<BS, false><<<persistent_grid(k_render_mega<BS, false>, BS, npix), BS, 0, stream>>>(v, p, d_out,
+                                                                                                      counter);
 }
 
 static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
@@ -1339,6 +1352,7 @@ struct zt_batch {
   uint64_t n = 0;
   uint64_t total_tiles = 0;
   uint32_t block_size = 128;
+  bool nee = true; /* some render of the batch samples lights */
   BatchItem* d_items = nullptr;
   unsigned int* d_counter = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1346,10 +1360,16 @@ struct zt_batch {
 
 namespace zt {
 
+template <int BS, bool kNee>
+static void launch_batch_kernel(const zt_batch* b, cudaStream_t st) {
+  k_render_batch<BS, kNee><<<persistent_grid(k_render_batch<BS, kNee>, BS, b->total_tiles * 32), BS, 0, st>>>(
+      b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
+}
+
 template <int BS>
 static void launch_batch_bs(const zt_batch* b, cudaStream_t st) {
-  k_render_batch<BS><<<persistent_grid(k_render_batch<BS>, BS, b->total_tiles * 32), BS, 0, st>>>(
-      b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
+  if (b->nee) launch_batch_kernel<BS, true>(b, st);
+  else launch_batch_kernel<BS, false>(b, st);
 }
 
 static void batch_free(zt_batch* b) {
@@ -1407,6 +1427,8 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
   b->n = n;
   b->total_tiles = tiles;
   b->block_size = bs ? bs : 128;
+  b->nee = false;
+  for (uint64_t k = 0; k < n; ++k) b->nee = b->nee || items[k].p.use_nee != 0;
   cudaError_t e = cudaGetDevice(&b->device);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_items, n * sizeof(BatchItem));
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(unsigned int));

@@ -600,12 +600,15 @@ ZT_D dv3 direct_light(const DevScene& sc, dv3 albedo, const Hit& hit, Rng& rng) 
   return vscale(vmul(albedo, lrad), scale);
 }
 
-/* traceWith, render.zig:61-102. */
+/* traceWith, render.zig:61-102.  kNee = false compiles light sampling out
+ * (for scenes where use_nee is false: no lights or light_sampling off); the
+ * path is then the reference's use_nee = false path, draw for draw. */
 struct TraceAux { int32_t first_prim; uint32_t path_len; };
 
-template <bool kAux>
-ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_depth, bool use_nee,
+template <bool kAux, bool kNee = true>
+ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_depth, bool use_nee_arg,
                     TraceAux* aux) {
+  const bool use_nee = kNee && use_nee_arg;
   dv3 radiance = V(0, 0, 0), throughput = V(1, 1, 1);
   dv3 prev_origin = V(0, 0, 0);
   double prev_pdf = 0;

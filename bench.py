@@ -41,10 +41,10 @@ NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 2.527835e9 / (1920 * 1080 * 8)}
 # issue slots used, lanes active per warp instruction, FP64 pipe activity.
 NCU_EXECUTION = {"triangle_heavy": {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
                                     "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
-                 "batch": {"issue_active_pct": 60.5, "lanes_per_warp_instruction": 14.23,
-                           "fp64_pipe_active_pct": 37.5, "l1_hit_pct": 71.9, "l2_hit_pct": 87.1}}
+                 "batch": {"issue_active_pct": 70.2, "lanes_per_warp_instruction": 14.23,
+                           "fp64_pipe_active_pct": 44.5, "l1_hit_pct": 82.9, "l2_hit_pct": 88.5}}
 # The batched launch, captured whole (rank 0's batch, one launch).
-NCU_DRAM_BYTES_BATCH = 0.661207e9 + 6.302831e9
+NCU_DRAM_BYTES_BATCH = 0.160607e9 + 1.138117e9
 
 
 def roofline_entry(work: dict, samples: int, kernel_ms: float, sms: int, traffic, traffic_note: str,

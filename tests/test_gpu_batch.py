@@ -77,3 +77,22 @@ def test_batch_rejects_bad_arguments():
     assert ei.value.name == "InvalidOptions"
     with pytest.raises(zt.ZigtraceError):
         zt.render_batch([s], [zt.Options(8, 8, 1, 4)], zt.GpuConfig(block_size=96))
+
+
+def test_batch_without_lights_matches_oracle():
+    """A batch in which no render samples lights runs the kernel instance
+    built without light sampling: sphere fields (no emitters) and lit fuzz
+    scenes with light_sampling off."""
+    items = scenes.batch_workload(count=6, spp=2, max_depth=16)
+    items += [(K.fuzz_scene(k), zt.Options(24, 16, 3, 12, seed=k, light_sampling=False)) for k in range(3)]
+    for s, _ in items:
+        s.build()
+    got = zt.render_batch([s for s, _ in items], [o for _, o in items])
+    for (s, o), img in zip(items, got):
+        if o.width * o.height > 64 * 64:
+            continue
+        want = O.OracleScene.from_scene(s).render(o.width, o.height, o.spp, o.max_depth, seed=o.seed,
+                                                  light_sampling=o.light_sampling)
+        assert img.pixels.tobytes() == want.tobytes()
+    for (s, o), img in zip(items, got):
+        assert img.pixels.tobytes() == zt.render(s, o).pixels.tobytes()

@@ -203,3 +203,13 @@ def test_fuzz_scenes_bit_exact(seed, mode):
     img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
     want = O.OracleScene.from_scene(scene).render(32, 20, 3, 12, seed=seed)
     assert img.tobytes() == want.tobytes()
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("seed", range(3))
+def test_fuzz_scenes_without_light_sampling_bit_exact(seed, mode):
+    scene = K.fuzz_scene(seed).build()
+    o = zt.Options(32, 20, 3, 12, seed=seed, light_sampling=False)
+    img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
+    want = O.OracleScene.from_scene(scene).render(32, 20, 3, 12, seed=seed, light_sampling=False)
+    assert img.tobytes() == want.tobytes()

@@ -396,33 +396,46 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
     plain_value = world * samples / (plain_ms / 1e3) / 1e6
 
     e2e = None
-    if not args.no_e2e:  # zt_render_batch with host buffers, scenes re-uploaded every step
+    if not args.no_e2e:  # zt_render_batch into pinned host buffers, scenes re-uploaded every step
+        import ctypes as C
+        from zigtrace_b200 import _native as N
+        pinned = [torch.empty(o.width * o.height * 3, dtype=torch.float64).pin_memory() for o in opts]
+        handles = (C.c_void_p * len(scs))(*[s.handle.value for s in scs])
+        recs = np.concatenate([o.record() for o in opts])
+        ptrs = (C.c_void_p * len(scs))(*[t.data_ptr() for t in pinned])
+        bcfg = cfg.record()
         times = []
         for i in range(args.warmup + args.steps):
             for s in scs:
                 s.release_device()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            zt.render_batch(scs, opts, cfg)
+            N.check(N.lib().zt_render_batch(handles, N.ptr(recs), len(scs), ptrs, N.ptr(bcfg)))
             if i >= args.warmup:
                 times.append(time.perf_counter() - t0)
         e2e_s = allmax(statistics.mean(times))
         e2e = {"value": round(world * samples / e2e_s / 1e6, 4), "unit": "Msamples/s",
                "h2d_bytes_per_step": sum(s.staging_bytes() for s in scs),
                "d2h_bytes_per_step": sum(o.width * o.height * 24 for o in opts)}
-        times = []  # the same 256 renders as one zt_render call each
+        same_e2e = all(torch.equal(x, t) for x, t in zip(batched_imgs, pinned))
+        times = []  # the same 256 renders as one zt_render_ex call each, into the same pinned buffers
+        pcfg = zt.GpuConfig(block_size=cfg.block_size).record()
+        orecs = [o.record() for o in opts]
         for i in range(args.warmup + args.steps):
             for s in scs:
                 s.release_device()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            for s, o in zip(scs, opts):
-                zt.render(s, o, zt.GpuConfig(block_size=cfg.block_size))
+            for s, r, t in zip(scs, orecs, pinned):
+                N.check(N.lib().zt_render_ex(s.handle, N.ptr(r), N.ptr(pcfg), C.c_void_p(t.data_ptr())))
             if i >= args.warmup:
                 times.append(time.perf_counter() - t0)
         plain_e2e_s = allmax(statistics.mean(times))
         e2e["plain_calls_value"] = round(world * samples / plain_e2e_s / 1e6, 4)
         e2e["batched_over_plain_calls"] = round(plain_e2e_s / e2e_s, 3)
+        e2e["host_buffers"] = "pinned"
+        e2e["identical_to_device_arm"] = bool(same_e2e and
+                                              all(torch.equal(x, t) for x, t in zip(batched_imgs, pinned)))
 
     cpu = None
     roofline = None

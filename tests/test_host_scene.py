@@ -100,3 +100,20 @@ def test_device_build_falls_back_to_the_host_tree_without_a_gpu(native_lib):
     assert not dev.built_on_device
     (dn, di), (hn, hi) = dev.bvh(), host.bvh()
     assert dn.tobytes() == hn.tobytes() and di.tobytes() == hi.tobytes()
+
+
+def test_device_entry_points_fail_loudly_without_a_gpu(native_lib):
+    """No CPU fallback: on a machine without a usable GPU every rendering
+    entry point returns a CUDA error instead of computing on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from zigtrace_b200 import scenes
+    s = scenes.cornell().build()
+    o = zt.Options(8, 8, 1, 4)
+    calls = [lambda: zt.render(s, o), lambda: zt.render_rgb8(s, o), lambda: zt.render_png(s, o),
+             lambda: zt.forward(s, o), lambda: zt.render_batch([s], [o])]
+    for call in calls:
+        with pytest.raises(zt.ZigtraceError) as ei:
+            call()
+        assert ei.value.name == "CudaError"

@@ -307,6 +307,7 @@ def b200_arm(args):
     # ---- CPU baseline and per-sample work from the oracle (rank 0, N=1)
     cpu = None
     work = None
+    queue_bytes = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         n_pix, dt, st = cpu_sample(scene, o, args.cpu_seconds, threads)
@@ -314,6 +315,7 @@ def b200_arm(args):
                "sample": f"{n_pix} random pixels x {o.spp} spp ({n_pix * o.spp} samples), oracle C restatement "
                          f"of the reference CPU renderer, {threads} threads, {dt:.1f} s"}
         work = workmodel.per_sample(st, o.spp, counts["nodes"] > 0)
+        queue_bytes = workmodel.wavefront_queue_bytes(st, o.spp)
 
     roofline = None
     if work is not None:
@@ -324,6 +326,13 @@ def b200_arm(args):
              if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
             "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
             NCU_EXECUTION.get(args.workload) if args.mode in (0, 1) else None)
+        if args.mode == 2:  # the wavefront form: path-state traffic through HBM against the copy peak
+            qbps = queue_bytes * samples / (kernel_ms / 1e3) / 1e9
+            roofline["queue"] = {"bytes_per_sample": round(queue_bytes, 1), "achieved_gbs": round(qbps, 1),
+                                 "peak_gbs": roofline["memory"]["peak_gbs"],
+                                 "frac": round(qbps / roofline["memory"]["peak_gbs"], 4),
+                                 "note": "path-state bytes of the wavefront kernels (workmodel.py), "
+                                         "oracle-counted rays, hits and shadow rays per sample"}
 
     line = {
         "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world,

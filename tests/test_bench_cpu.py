@@ -74,3 +74,12 @@ def test_work_model_from_oracle_counters():
               workmodel.FLOP_SHADE * st["hits"] + workmodel.FLOP_NEE * st["nee_samples"]) / st["samples"]
     assert w["flop"] == pytest.approx(expect)
     assert w["bytes"] > workmodel.BYTES_PIXEL / 4
+
+
+def test_wavefront_queue_bytes():
+    st = {"samples": 100, "ext_rays": 157, "hits": 61, "shadow_rays": 33}
+    b = workmodel.wavefront_queue_bytes(st, 4)
+    want = (workmodel.WF_BYTES_SAMPLE + (workmodel.WF_BYTES_RAY * 157 + workmodel.WF_BYTES_HIT * 61 +
+                                         workmodel.WF_BYTES_SHADOW * 33) / 100 + workmodel.BYTES_PIXEL / 4)
+    assert b == pytest.approx(want)
+    assert 700 < b < 1000  # the 1M-triangle workload's counters give about 830 bytes per sample

@@ -50,3 +50,27 @@ def per_sample(stats: dict, spp: int, has_bvh: bool = True) -> dict:
         "box_tests": stats["slab_tests"] / n,
         "prim_tests": prim_tests / n,
     }
+
+
+# Path-state bytes the wavefront form moves through HBM (wavefront.cuh's
+# WfState, f64 SoA), counted from its kernels:
+#   per sample   start + finish: ray, throughput, radiance, previous hit,
+#                depth, flags, RNG state, sample index, pixel sum, queue push
+#   per ray      k_wf_extend (queue index, ray in; hit t and id out) and the
+#                part of k_wf_shade every ray pays (RNG, ray, throughput,
+#                radiance, hit id in; radiance and RNG out)
+#   per hit      hit t, depth; the scattered ray, throughput, previous hit,
+#                depth and queue push written back
+#   per shadow   the light sample written by k_wf_shade (13 doubles + push)
+#                and k_wf_shadow's reads, radiance update and flags
+WF_BYTES_SAMPLE = 256
+WF_BYTES_RAY = 64 + 136 + 56
+WF_BYTES_HIT = 8 + 4 + 116
+WF_BYTES_SHADOW = 108 + 160
+
+
+def wavefront_queue_bytes(stats: dict, spp: int) -> float:
+    """Path-state bytes per sample of the wavefront form, from oracle counters."""
+    n = max(stats["samples"], 1)
+    return (WF_BYTES_SAMPLE + (WF_BYTES_RAY * stats["ext_rays"] + WF_BYTES_HIT * stats["hits"] +
+                               WF_BYTES_SHADOW * stats["shadow_rays"]) / n + BYTES_PIXEL / spp)

@@ -86,6 +86,8 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size in seconds")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="default workload only: skip the batch and diff sub-objects")
     p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
     p.add_argument("--capacity", type=int, default=0, help="zt_gpu_config.queue_capacity (wavefront)")
     return p.parse_args()
@@ -115,11 +117,11 @@ def describe(name, scene, o, counts):
 
 
 # ------------------------------------------------------------- CPU leg ----
-def cpu_sample(scene, o, seconds: float, threads: int, rng_seed: int = 1):
+def cpu_sample(scene, o, seconds: float, threads: int, rng_seed: int = 1, oscene=None):
     """Oracle render of random pixels of the workload, sized to ~seconds."""
     import numpy as np
     import oracle as O
-    os_ = O.OracleScene.from_scene(scene)
+    os_ = oscene if oscene is not None else O.OracleScene.from_scene(scene)
     npix = o.width * o.height
     rng = np.random.default_rng(rng_seed)
     n = 64
@@ -139,13 +141,13 @@ def reference_arm(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    scene, o = workload(args.workload, args.spp)
-    counts_scene = scene.build().counts()
-    per_step = max(args.cpu_seconds / 3.0, 2.0)
-    n_pix, _, _ = cpu_sample(scene, o, per_step, threads)  # calibration
+    scene, o = workload(args.workload, args.spp)  # NumPy arrays only: the product library is never loaded
     import numpy as np
     import oracle as O
     os_ = O.OracleScene.from_scene(scene)
+    counts_scene = os_.counts()
+    per_step = max(args.cpu_seconds / 3.0, 2.0)
+    n_pix, _, _ = cpu_sample(scene, o, per_step, threads, oscene=os_)  # calibration
     rng = np.random.default_rng(7)
     times = []
     for i in range(args.warmup + args.steps):
@@ -206,6 +208,37 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- GPU leg ----
+def e2e_breakdown(scene, o, gcfg, d_out, pinned, args, allmax) -> dict:
+    """Where an end-to-end step's time goes: the same work as separate public
+    calls, each timed on the host after a device synchronisation -- scene
+    upload (device allocation from the library's pool + host-to-device copy),
+    render into device memory, framebuffer read-back into pinned memory."""
+    import torch
+
+    import zigtrace_b200 as zt
+    up, rend, back = [], [], []
+    for i in range(args.warmup + args.steps):
+        scene.release_device()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scene.upload()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        zt.render_device(scene, o, d_out.data_ptr(), 0, gcfg)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        pinned.copy_(d_out)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        if i >= args.warmup:
+            up.append(t1 - t0)
+            rend.append(t2 - t1)
+            back.append(t3 - t2)
+    return {"upload": round(1e3 * allmax(statistics.mean(up)), 3),
+            "render": round(1e3 * allmax(statistics.mean(rend)), 3),
+            "readback": round(1e3 * allmax(statistics.mean(back)), 3)}
+
+
 def b200_arm(args):
     import numpy as np
     import torch
@@ -234,10 +267,14 @@ def b200_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    if args.workload == "batch":
-        return batch_arm(args, world, rank, local_rank, barrier, allmax)
-    if args.workload == "diff":
-        return diff_arm(args, world, rank, local_rank, barrier, allmax)
+    if args.workload in ("batch", "diff"):
+        arm = batch_arm if args.workload == "batch" else diff_arm
+        line = arm(args, world, rank, local_rank, barrier, allmax)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     scene, o = workload(args.workload, args.spp)
     o.seed = o.seed + rank  # each rank renders its own frame
     scene.build(device=True)  # the same tree as the host build (zt_scene_build_device)
@@ -301,7 +338,11 @@ def b200_arm(args):
                 times.append(t1 - t0)
         e2e_s = allmax(statistics.mean(times))
         e2e = {"value": round(world * samples / e2e_s / 1e6, 4), "unit": "Msamples/s",
-               "h2d_bytes_per_step": scene.staging_bytes(), "d2h_bytes_per_step": npix * 3 * 8}
+               "h2d_bytes_per_step": scene.staging_bytes(), "d2h_bytes_per_step": npix * 3 * 8,
+               "ms_per_step": round(1e3 * e2e_s, 3), "host_buffers": "pinned",
+               "breakdown_ms": e2e_breakdown(scene, o, gcfg, out, pinned, args, allmax),
+               "identical_to_device_arm": bool((pinned.numpy() == img).all())}
+        e2e["breakdown_ms"]["unaccounted"] = round(1e3 * e2e_s - sum(e2e["breakdown_ms"].values()), 3)
         scene.upload()
 
     # ---- CPU baseline and per-sample work from the oracle (rank 0, N=1)
@@ -345,6 +386,16 @@ def b200_arm(args):
                                  "device_ms": round(scene.build_ms, 2) if scene.build_ms else None}},
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
     }
+    if not args.no_extras:
+        # the other two parts of the metric, each with its own clocks, e2e and
+        # timing: batched vs plain launches, and backward vs forward time
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup, sub.spp = min(args.steps, 10), 3, 0
+        del out, flush
+        torch.cuda.empty_cache()
+        line["batch"] = batch_arm(sub, world, rank, local_rank, barrier, allmax)
+        torch.cuda.empty_cache()
+        line["diff"] = diff_arm(sub, world, rank, local_rank, barrier, allmax)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -495,11 +546,8 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
         "batched_over_plain": round(plain_ms / batch_ms, 3), "identical_images": bool(same),
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     batch.close()
-    if world > 1:
-        dist.destroy_process_group()
+    return line
 
 
 def diff_arm(args, world, rank, local_rank, barrier, allmax):
@@ -544,8 +592,11 @@ def diff_arm(args, world, rank, local_rank, barrier, allmax):
 
     img = fwd(theta0)
     d_img = 2.0 * (img - target_img)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     fwd_s = timed(lambda: fwd(theta0))
     bwd_s = timed(lambda: zt.backward(scene, o, d_img, theta0))
+    clk = clocks.stop()
     grad = zt.backward(scene, o, d_img, theta0)
 
     h, errs, fd_vals = 1e-3, [], {}
@@ -594,12 +645,9 @@ def diff_arm(args, world, rank, local_rank, barrier, allmax):
                              "mean_abs_param_err_end": param_err},
         "e2e": {"value": round(world * samples / fwd_s / 1e6, 4), "unit": "Msamples/s",
                 "h2d_bytes_per_step": int(theta0.nbytes), "d2h_bytes_per_step": o.width * o.height * 24},
-        "gpu_launches": args.steps, "roofline": None, "cpu_baseline": None,
+        "gpu_launches": args.steps, "clocks": clk, "roofline": None, "cpu_baseline": None,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    return line
 
 
 def main():

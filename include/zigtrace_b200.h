@@ -173,10 +173,19 @@ zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu
  * zt_backward takes dL/dimage (width*height*3) and writes dL/dcolors
  * (n_materials*3), replaying each path from its RNG stream (no tape).
  * Gradients are accumulated with atomics, so their last bits may vary
- * between runs. */
+ * between runs.
+ * Memory: zt_forward keeps every sample's primal radiance on the device for
+ * the next zt_backward with the same options, colours, camera and
+ * background (24 bytes per sample of the whole image: 403 MB at 512x512x64)
+ * when that fits the scene's primal cache limit (default 1 GiB); above the
+ * limit nothing is kept and zt_backward traces the primal itself, which
+ * gives the same gradients. */
 zt_status zt_forward(zt_scene* scene, const zt_options* opts, const double* colors, double* out_rgb);
 zt_status zt_backward(zt_scene* scene, const zt_options* opts, const double* colors, const double* d_image,
                       double* d_colors);
+/* Largest primal cache (bytes) zt_forward may keep for this scene; 0 keeps
+ * none.  Lowering it below the cache held now frees that cache. */
+zt_status zt_scene_set_primal_cache_limit(zt_scene* scene, uint64_t max_bytes);
 /* The same for the image rows [row_begin, row_end) (one band of a frame
  * sharded across GPUs): out_rgb and d_image hold the band's rows only,
  * d_colors the band's share of the gradient (the shares of all bands sum to
@@ -207,11 +216,12 @@ zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint6
                           const zt_gpu_config* cfg);
 
 /* Allocation-free render, for callers that must not allocate device memory
- * while rendering: a frame loop recorded into a CUDA graph by stream capture
- * (a cudaMalloc there breaks the capture), or an engine or service whose own
- * pool owns the GPU's memory after start-up.  It has no counterpart in the
- * reference.  The scene must already be resident (zt_scene_upload, which
- * allocates, belongs at set-up).  The call uses no memory beyond the scene but
+ * while rendering: an engine or service that hands the GPU's memory to its
+ * own pool at start-up and fails or stalls on any allocation made behind its
+ * back afterwards, or a frame loop that cannot afford the device-wide
+ * synchronisation a cudaMalloc/cudaFree pair can cost.  It has no
+ * counterpart in the reference.  The scene must already be resident
+ * (zt_scene_upload, which allocates, belongs at set-up).  The call uses no memory beyond the scene but
  * a 6 MiB scratch array compiled into the library (held by every GPU that
  * loads it, for the life of the process): the work counter and a staging
  * framebuffer of at most ZT_NOALLOC_MAX_PIXELS pixels; larger images are
@@ -220,7 +230,9 @@ zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint6
  * synchronising `stream` (a cudaStream_t, NULL = legacy default stream).
  * The first call on a device looks up the scratch's device address (and may
  * load the library's GPU code there): make it before any stream capture.
- * All calls share the scratch, so calls whose GPU work overlaps race. */
+ * The address is looked up again when the device's context changes (after
+ * cudaDeviceReset, for instance).  All calls share the scratch and it keeps
+ * the last call's contents, so calls whose GPU work overlaps race. */
 #define ZT_NOALLOC_MAX_PIXELS (512u * 512u)
 #define ZT_NOALLOC_FB_OFFSET 256u
 zt_status zt_render_noalloc(zt_scene* scene, const zt_options* opts, double* out_rgb, void* stream);

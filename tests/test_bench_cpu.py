@@ -40,6 +40,20 @@ def test_reference_arm_prints_one_contract_line():
     assert "workload" in d["config"]
 
 
+def test_reference_arm_never_loads_the_product_library():
+    """The reference arm times the oracle only: the product's shared library
+    must not even be mapped into its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'cornell', "
+            "'--steps', '1', '--warmup', '0', '--cpu-seconds', '1']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_LIB_MAPPED' if 'libzt_b200' in maps else 'PRODUCT_LIB_ABSENT'); "
+            "print('ORACLE_MAPPED' if 'libzt_oracle' in maps else 'ORACLE_ABSENT')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PRODUCT_LIB_ABSENT" in r.stdout and "ORACLE_MAPPED" in r.stdout
+
+
 def test_reference_arm_other_ranks_print_nothing():
     r = _run_reference({"RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]

@@ -163,3 +163,46 @@ def test_forward_at_own_colors_on_fuzz_scenes(seed):
     scene = K.fuzz_scene(seed).build()
     o = zt.Options(32, 20, 3, 12, seed=seed)
     assert zt.forward(scene, o).pixels.tobytes() == zt.render(scene, o).pixels.tobytes()
+
+
+def test_backward_after_a_second_view_uses_its_own_primal():
+    """Forward view A, forward view B, backward A: the primal kept by the last
+    forward belongs to view B, so the backward of A must not reuse it; the
+    gradient equals backward A computed with no cache at all."""
+    scene, _, o = small()
+    theta = np.array([m["color"] for m in scene.materials])
+    w = _weights(o)
+    view_a = scene.camera
+    view_b = zt.CameraConfig(look_from=(300, 250, -700), look_at=(270, 270, 0), vfov=42)
+    zt.forward(scene, o, theta)                      # A
+    scene.camera = view_b
+    zt.forward(scene, o, theta)                      # B: its primal replaces A's
+    scene.camera = view_a
+    warm = zt.backward(scene, o, w, theta)           # A again
+    scene.set_primal_cache_limit(0)                  # no cache: the backward traces its own primal
+    cold = zt.backward(scene, o, w, theta)
+    tol = dict(rtol=1e-9, atol=1e-12 * np.abs(cold).max())  # atomics add in varying order
+    np.testing.assert_allclose(warm, cold, **tol)
+    scene.background = zt.Background.solid((0.2, 0.3, 0.4))  # the same for a background change
+    scene.set_primal_cache_limit(1 << 30)
+    zt.forward(scene, o, theta)
+    scene.background = zt.Background.solid((0.0, 0.0, 0.0))
+    np.testing.assert_allclose(zt.backward(scene, o, w, theta), cold, **tol)
+
+
+def test_primal_cache_off_at_full_hd_matches_cached():
+    """1920x1080x64 (3.2 GB of primal radiance, above the default 1 GiB cache
+    limit, so the default backward recomputes the primal) against the same
+    backward with the cache raised to hold it."""
+    scene, target = scenes.cornell_diff()
+    scene.build()
+    o = zt.Options(1920, 1080, 64, 8)
+    theta = np.array([m["color"] for m in scene.materials])
+    w = np.random.default_rng(9).uniform(-1, 1, (o.width * o.height, 3))
+    img = zt.forward(scene, o, theta).pixels
+    recomputed = zt.backward(scene, o, w, theta)
+    scene.set_primal_cache_limit(4 << 30)
+    assert zt.forward(scene, o, theta).pixels.tobytes() == img.tobytes()
+    cached = zt.backward(scene, o, w, theta)
+    np.testing.assert_allclose(cached, recomputed, rtol=1e-9, atol=1e-12 * np.abs(recomputed).max())
+    assert np.abs(cached).max() > 0

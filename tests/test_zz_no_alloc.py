@@ -1,6 +1,8 @@
 """zt_render_noalloc: the render entry point for callers that must not
-allocate device memory while rendering (a frame loop recorded by CUDA stream
-capture, or an engine whose own pool owns the GPU's memory after start-up).
+allocate device memory while rendering (an engine or service whose own pool
+takes the GPU's memory at start-up and fails or stalls on allocations made
+behind its back, or a frame loop that cannot afford an allocator's
+device-wide synchronisation).
 
 It is checked through the C ABI against the existing entry point, zt_render,
 on two calls in a row.  The tolerance is the one every render test here

@@ -81,6 +81,7 @@ SIGNATURES = {
     "zt_backward": (_i32, [_P, _P, _P, _P, _P]),
     "zt_forward_rows": (_i32, [_P, _P, _u64, _u64, _P, _P]),
     "zt_backward_rows": (_i32, [_P, _P, _u64, _u64, _P, _P, _P]),
+    "zt_scene_set_primal_cache_limit": (_i32, [_P, _u64]),
     "zt_batch_create": (_i32, [_P, _P, _u64, _P, _P, _u32, C.POINTER(_P)]),
     "zt_batch_launch": (_i32, [_P, _P]),
     "zt_batch_destroy": (None, [_P]),

@@ -335,6 +335,11 @@ class Scene:
         if self._handle is not None:
             N.check(N.lib().zt_scene_release_device(self._handle))
 
+    def set_primal_cache_limit(self, max_bytes: int) -> None:
+        """Largest per-sample primal cache ``forward`` may keep for
+        ``backward`` (0 keeps none; the backward then traces the primal)."""
+        N.check(N.lib().zt_scene_set_primal_cache_limit(self.handle, int(max_bytes)))
+
     def staging_bytes(self) -> int:
         """Bytes one upload copies host-to-device (from pinned memory)."""
         b = C.c_uint64()

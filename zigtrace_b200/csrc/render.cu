@@ -50,9 +50,11 @@ struct zt_wavefront_cache {
   unsigned char key[sizeof(zt::DevScene) + sizeof(zt::RenderParams) + 2 * sizeof(void*)] = {};
 };
 
-/* The per-sample primal radiance of the last zt_forward, with the options
- * and parameters it was computed for; a zt_backward with the same ones
- * replays paths against it instead of recomputing the primal. */
+/* The per-sample primal radiance of the last zt_forward, with everything it
+ * depends on: options, parameters, camera and background.  A zt_backward
+ * with the same ones replays paths against it instead of recomputing the
+ * primal; any difference (another view rendered in between, for instance)
+ * makes the backward recompute. */
 struct zt_diff_cache {
   double* L = nullptr;
   size_t cap = 0; /* doubles */
@@ -60,6 +62,8 @@ struct zt_diff_cache {
   zt_options opts{};
   uint64_t row0 = 0, rows = 0; /* the band the cached samples belong to */
   std::vector<double> theta;
+  zt_camera_config camera{};
+  zt_background background{};
 };
 
 struct zt_device_buffers {
@@ -84,19 +88,65 @@ static zt_status cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
+/* Stream-ordered allocations from one memory pool per device, for the
+ * buffers the synchronous entry points need per call or per upload (the
+ * scene block, framebuffers).  Memory freed into the pool stays reserved
+ * for the next allocation, up to kPoolKeepBytes across synchronisations, so
+ * re-uploading a scene or rendering into host buffers frame after frame
+ * costs no cudaMalloc/cudaFree pair (each maps or unmaps device pages and
+ * synchronises the device). */
+constexpr uint64_t kPoolKeepBytes = 4ull << 30;
+static std::mutex g_pool_mutex;
+static cudaMemPool_t g_pools[256] = {};
+
+static zt_status device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= 256) return fail(ZT_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    ZT_CUDA(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = kPoolKeepBytes;
+    ZT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return ZT_OK;
+}
+
+static zt_status pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
+  cudaMemPool_t pool = nullptr;
+  zt_status rc = device_pool(&pool);
+  if (rc != ZT_OK) return rc;
+  ZT_CUDA(cudaMallocFromPoolAsync(p, bytes > 0 ? bytes : 256, pool, st), what);
+  return ZT_OK;
+}
+
+static void pool_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
 void release_device(zt_scene* s) {
   zt_device_buffers* d = s->device;
   if (!d) return;
   int cur = -1;
   cudaGetDevice(&cur);
   if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
-  if (d->wf.done) cudaEventSynchronize(d->wf.done);
+  /* work on any stream may still read the scene: wait for it, as cudaFree would */
+  cudaDeviceSynchronize();
   if (d->wf.exec) cudaGraphExecDestroy(d->wf.exec);
   if (d->wf.done) cudaEventDestroy(d->wf.done);
   cudaFree(d->wf.block);
   cudaFree(d->diff.L);
-  cudaFree(d->block);
-  cudaFree(d->counter);
+  pool_free(d->block, 0);
+  pool_free(d->counter, 0);
+  cudaStreamSynchronize(0);
   if (d->device >= 0 && d->device != cur) cudaSetDevice(cur);
   delete d;
   s->device = nullptr;
@@ -176,9 +226,14 @@ static zt_status upload(zt_scene* s) {
   if (!d) return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory");
   d->device = dev;
   s->device = d;
-  cudaError_t e = cudaMalloc(&d->block, h->bytes);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&d->counter, 4 * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMemcpy(d->block, h->pinned, h->bytes, cudaMemcpyHostToDevice);
+  zt_status arc = pool_alloc(&d->block, h->bytes, 0, "allocate the scene block");
+  if (arc == ZT_OK) arc = pool_alloc((void**)&d->counter, 4 * sizeof(unsigned int), 0, "allocate the work counter");
+  if (arc != ZT_OK) {
+    release_device(s);
+    return arc;
+  }
+  cudaError_t e = cudaMemcpyAsync(d->block, h->pinned, h->bytes, cudaMemcpyHostToDevice, 0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     release_device(s);
     return cuda_fail(e, "upload scene");
@@ -878,14 +933,15 @@ zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cf
   if (rc != ZT_OK) return rc;
   const size_t bytes = (size_t)(o->width * o->height * 3) * sizeof(double);
   double* d_out = nullptr;
-  ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer");
+  if ((rc = pool_alloc((void**)&d_out, bytes, 0, "allocate framebuffer")) != ZT_OK) return rc;
   rc = launch_render(s, o, cfg, d_out, 0);
   if (rc == ZT_OK) {
-    cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) rc = cuda_fail(e, "render / copy framebuffer");
     else rc = wavefront_status(s, cfg);
   }
-  cudaFree(d_out);
+  pool_free(d_out, 0);
   return rc;
 }
 
@@ -913,7 +969,9 @@ static zt_status render_encoded(zt_scene* s, const zt_options* o, const zt_gpu_c
   const size_t fb_bytes = up(npix * 3 * sizeof(double)), rgb_bytes = up(npix * 3);
   const size_t png_bytes = png ? up(L.total) : 0, scratch_bytes = png ? up(png_scratch_bytes(L)) : 0;
   unsigned char* block = nullptr;
-  ZT_CUDA(cudaMalloc((void**)&block, fb_bytes + rgb_bytes + png_bytes + scratch_bytes), "allocate output buffers");
+  if ((rc = pool_alloc((void**)&block, fb_bytes + rgb_bytes + png_bytes + scratch_bytes, 0,
+                       "allocate output buffers")) != ZT_OK)
+    return rc;
   double* d_fb = reinterpret_cast<double*>(block);
   uint8_t* d_rgb = block + fb_bytes;
   uint8_t* d_png = d_rgb + rgb_bytes;
@@ -921,11 +979,12 @@ static zt_status render_encoded(zt_scene* s, const zt_options* o, const zt_gpu_c
   if (rc == ZT_OK) rc = launch_encode_rgb8(d_fb, 3 * npix, tonemap, gamma, exposure, d_rgb, 0);
   if (rc == ZT_OK && png) rc = launch_png(d_rgb, L, d_png, d_png + png_bytes, 0);
   if (rc == ZT_OK) {
-    const cudaError_t e = cudaMemcpy(out, png ? d_png : d_rgb, out_bytes, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(out, png ? d_png : d_rgb, out_bytes, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) rc = cuda_fail(e, "copy encoded image");
     else rc = wavefront_status(s, cfg);
   }
-  cudaFree(block);
+  pool_free(block, 0);
   return rc;
 }
 
@@ -956,13 +1015,14 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
     return ZT_OK;
   }
   double* d_out = nullptr;
-  ZT_CUDA(cudaMalloc((void**)&d_out, bytes), "allocate framebuffer band");
+  if ((rc = pool_alloc((void**)&d_out, bytes, 0, "allocate framebuffer band")) != ZT_OK) return rc;
   rc = launch_mega(s, p, 0, d_out, s->pilot_valid && s->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested, 0);
   if (rc == ZT_OK) {
-    const cudaError_t e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) rc = cuda_fail(e, "render rows / copy framebuffer band");
   }
-  cudaFree(d_out);
+  pool_free(d_out, 0);
   return rc;
 }
 
@@ -1258,15 +1318,19 @@ zt_status zt_forward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, 
   double *d_theta = nullptr, *d_out = nullptr;
   if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
   /* keep every sample's primal radiance for a following zt_backward (24 bytes
-   * per sample, indexed by image pixel); if that memory is not available the
-   * backward recomputes it */
+   * per sample of the whole image, indexed by image pixel) when that fits the
+   * scene's primal cache limit; above it, or if the memory is not available,
+   * the backward recomputes the primal from the RNG stream */
   const size_t n_l = (size_t)(p.width * p.height * p.spp) * 3;
-  if (cache.cap < n_l) {
+  const bool keep = (uint64_t)n_l * sizeof(double) <= s->primal_cache_limit;
+  if (!keep || cache.cap < n_l) {
     cudaFree(cache.L);
     cache.L = nullptr;
     cache.cap = 0;
-    if (cudaMalloc((void**)&cache.L, n_l * sizeof(double)) == cudaSuccess) cache.cap = n_l;
-    else cudaGetLastError();
+    if (keep) {
+      if (cudaMalloc((void**)&cache.L, n_l * sizeof(double)) == cudaSuccess) cache.cap = n_l;
+      else cudaGetLastError();
+    }
   }
   cudaError_t e = cudaMalloc((void**)&d_out, bytes);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
@@ -1285,6 +1349,22 @@ zt_status zt_forward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, 
     cache.row0 = p.row0;
     cache.rows = p.rows;
     cache.theta = th;
+    cache.camera = s->camera;
+    cache.background = s->background;
+  }
+  return ZT_OK;
+}
+
+zt_status zt_scene_set_primal_cache_limit(zt_scene* s, uint64_t max_bytes) {
+  if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_set_primal_cache_limit: NULL scene");
+  s->primal_cache_limit = max_bytes;
+  if (s->device && s->device->diff.cap * sizeof(double) > max_bytes) { /* drop a cache above the new limit */
+    zt_diff_cache& c = s->device->diff;
+    cudaDeviceSynchronize();
+    cudaFree(c.L);
+    c.L = nullptr;
+    c.cap = 0;
+    c.valid = false;
   }
   return ZT_OK;
 }
@@ -1312,7 +1392,9 @@ zt_status zt_backward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin,
   const std::vector<double> th = theta_host(s, colors);
   const zt_diff_cache& cache = s->device->diff;
   const bool cached = cache.valid && same_render(cache.opts, *o) && cache.theta == th && cache.row0 <= p.row0 &&
-                      p.row0 + p.rows <= cache.row0 + cache.rows;
+                      p.row0 + p.rows <= cache.row0 + cache.rows &&
+                      memcmp(&cache.camera, &s->camera, sizeof s->camera) == 0 &&
+                      memcmp(&cache.background, &s->background, sizeof s->background) == 0;
   const double* sample_L = cached ? cache.L : nullptr;
   const size_t img_bytes = (size_t)(p.rows * o->width * 3) * sizeof(double);
   double *d_theta = nullptr, *d_img = nullptr, *d_grad = nullptr;
@@ -1496,11 +1578,10 @@ zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint6
 /* ----------------------------------------------- Allocation-free render ---- */
 /*
  * zt_render_noalloc is for callers that must not allocate device memory once
- * they are rendering: a frame loop recorded inside CUDA stream capture (a
- * cudaMalloc there is not a stream operation and breaks the capture), an
- * engine or service that hands every byte of the GPU to its own pool at
- * start-up and forbids allocations afterwards, or a real-time loop that cannot
- * afford the allocator's synchronisation.  The scene is uploaded once at
+ * they are rendering: an engine or service that hands every byte of the GPU
+ * to its own pool at start-up and forbids allocations afterwards, or a
+ * real-time loop that cannot afford the allocator's synchronisation.  The
+ * scene is uploaded once at
  * set-up (zt_scene_upload allocates; do it before the loop).  Per call, the
  * only device memory used beyond the uploaded scene is the scratch below:
  * the persistent grid's work counter and a staging framebuffer for at most
@@ -1539,18 +1620,52 @@ __global__ void __launch_bounds__(128, 7) k_render_mega_noalloc(DevScene sc, Ren
  * memory: its device address is looked up once per device, with that device
  * current, and cached.  The lookup may load this library's GPU code on that
  * device, which is why the first call on a device belongs before any stream
- * capture. */
+ * capture.  The address belongs to the device's context: after a
+ * cudaDeviceReset the module is loaded again, possibly elsewhere, so each
+ * cached address carries the unique id of the context it was looked up in
+ * (cuCtxGetId, reached through the runtime's driver entry point) and is
+ * looked up again when the current context's id differs. */
 static std::mutex g_noalloc_mutex;
 static unsigned char* g_noalloc_ptr[256] = {};
+static unsigned long long g_noalloc_ctx[256] = {};
+
+typedef int (*ZtCtxGetCurrent)(void** ctx);
+typedef int (*ZtCtxGetId)(void* ctx, unsigned long long* id);
+
+/* Id of the current context, 0 when the driver cannot tell. */
+static unsigned long long current_context_id() {
+  static ZtCtxGetCurrent get_current = nullptr;
+  static ZtCtxGetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<ZtCtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<ZtCtxGetId>(f);
+    cudaGetLastError();
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 static zt_status noalloc_scratch(int dev, unsigned char** out) {
   if (dev < 0 || dev >= 256) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_noalloc: device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
     g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    g_noalloc_ctx[dev] = ctx;
   }
   *out = g_noalloc_ptr[dev];
   return ZT_OK;

@@ -58,6 +58,7 @@ struct zt_scene {
   bool pilot_valid = false;             /* mean_path is current for this build, camera and background */
   double mean_path = 0;                 /* mean path length of the pilot that ZT_MODE_AUTO reads */
   zt_host_staging* staging = nullptr;   /* pinned flattened copy, owned */
+  uint64_t primal_cache_limit = 1ull << 30; /* bytes zt_forward may keep for zt_backward */
 };
 
 namespace zt {

@@ -90,6 +90,8 @@ def parse_args():
                    help="default workload only: skip the batch and diff sub-objects")
     p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
     p.add_argument("--capacity", type=int, default=0, help="zt_gpu_config.queue_capacity (wavefront)")
+    p.add_argument("--precision", choices=["exact", "fast"], default="fast",
+                   help="zt_gpu_config.precision of the measured render (exact = the verification build)")
     return p.parse_args()
 
 
@@ -117,6 +119,23 @@ def describe(name, scene, o, counts):
 
 
 # ------------------------------------------------------------- CPU leg ----
+def measured_image_error(scene, o, img, threads: int, n_pixels: int = 4000, rng_seed: int = 11) -> dict:
+    """The measured frame against the oracle at the same seed on random
+    pixels: per-channel relative RMSE and mean luminance in Monte Carlo
+    standard errors (oracle/agreement.py)."""
+    import numpy as np
+    import oracle as O
+    from oracle.agreement import image_agreement
+    rng = np.random.default_rng(rng_seed)
+    pix = np.unique(rng.integers(0, o.width * o.height, n_pixels)).astype(np.uint64)
+    want, m2 = O.OracleScene.from_scene(scene).render_pixels_moments(o.width, o.height, o.spp, o.max_depth, pix,
+                                                                     threads=threads, seed=o.seed,
+                                                                     light_sampling=o.light_sampling)
+    a = image_agreement(img.reshape(-1, 3)[pix.astype(np.int64)], want, m2, o.spp)
+    a["pixels"] = int(len(pix))
+    return a
+
+
 def cpu_sample(scene, o, seconds: float, threads: int, rng_seed: int = 1, oscene=None):
     """Oracle render of random pixels of the workload, sized to ~seconds."""
     import numpy as np
@@ -280,7 +299,8 @@ def b200_arm(args):
     scene.build(device=True)  # the same tree as the host build (zt_scene_build_device)
     counts = scene.counts()
     scene.upload()
-    gcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity)
+    prec = zt.PRECISION_FAST if args.precision == "fast" else zt.PRECISION_EXACT
+    gcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity, precision=prec)
     npix = o.width * o.height
     samples = npix * o.spp
     out = torch.empty(npix * 3, dtype=torch.float64, device="cuda")
@@ -321,6 +341,32 @@ def b200_arm(args):
     img = out.cpu().numpy()
     assert np.isfinite(img).all(), "non-finite pixel in the framebuffer"
 
+    verification = None
+    if prec == zt.PRECISION_FAST and not args.no_extras:
+        # the verification build (bit-identical to the reference algorithm) on
+        # the same frame, timed the same way
+        vcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity, precision=zt.PRECISION_EXACT)
+        for _ in range(args.warmup):
+            flush.zero_()
+            zt.render_device(scene, o, out.data_ptr(), stream.cuda_stream, vcfg)
+        torch.cuda.synchronize()
+        barrier()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        v0.record(stream)
+        for _ in range(args.steps):
+            flush.zero_()
+            zt.render_device(scene, o, out.data_ptr(), stream.cuda_stream, vcfg)
+        v1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        v_ms = allmax(v0.elapsed_time(v1)) / args.steps
+        exact_img = out.cpu().numpy()
+        verification = {"precision": "exact", "value": round(world * samples / (v_ms / 1e3) / 1e6, 4),
+                        "unit": "Msamples/s", "ms_per_step": round(v_ms, 3),
+                        "fast_over_exact": round(v_ms / ms_per_step, 3),
+                        "identical_pixels_fast_vs_exact": float((exact_img.reshape(-1, 3) ==
+                                                                 img.reshape(-1, 3)).all(axis=1).mean())}
+
     # ---- e2e through the public C-ABI call with host buffers
     e2e = None
     if not args.no_e2e:
@@ -349,6 +395,7 @@ def b200_arm(args):
     cpu = None
     work = None
     queue_bytes = None
+    image_error = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         n_pix, dt, st = cpu_sample(scene, o, args.cpu_seconds, threads)
@@ -357,6 +404,7 @@ def b200_arm(args):
                          f"of the reference CPU renderer, {threads} threads, {dt:.1f} s"}
         work = workmodel.per_sample(st, o.spp, counts["nodes"] > 0)
         queue_bytes = workmodel.wavefront_queue_bytes(st, o.spp)
+        image_error = measured_image_error(scene, o, img, threads)
 
     roofline = None
     if work is not None:
@@ -381,10 +429,12 @@ def b200_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
                    "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][args.mode],
+                   "precision": args.precision,
                    "sharding": "one frame per rank (seed = rank), no collective",
                    "bvh_build": {"on_device": scene.built_on_device,
                                  "device_ms": round(scene.build_ms, 2) if scene.build_ms else None}},
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+        "image_error": image_error, "verification_build": verification,
     }
     if not args.no_extras:
         # the other two parts of the metric, each with its own clocks, e2e and

@@ -86,11 +86,23 @@ typedef struct { zt_shape shape; zt_vec3 radiance; double weight; } zt_light;
  * length of a 64x64, 1-spp pilot traced at zt_scene_upload is at least 3,
  * else MEGAKERNEL.  All modes give bit-identical images. */
 enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_MEGAKERNEL_REGEN = 3 };
+/* ZT_PRECISION_EXACT (the default) is the verification build of the path:
+ * every operation is the reference's f64 operation in the reference's order,
+ * so images are bit-identical to the reference algorithm's.
+ * ZT_PRECISION_FAST tests BVH boxes in single precision against conservative
+ * (outward-rounded, widened) copies of the f64 boxes; primitive tests, hit
+ * records and shading stay the reference's f64 operations.  It visits every
+ * BVH leaf the exact walk visits (and some more), so the closest hit differs
+ * only on exact ties and rays that graze a box edge: images agree with the
+ * exact ones to far below Monte Carlo noise, though not bit for bit.  Used by
+ * the megakernel modes and the batch; scenes whose leaves hold more than 15
+ * primitives or whose bounds or camera exceed 1e7 in magnitude render exact. */
+enum { ZT_PRECISION_EXACT = 0, ZT_PRECISION_FAST = 1 };
 typedef struct {
   uint32_t mode;           /* ZT_MODE_* */
   uint32_t block_size;     /* threads per block, 0 = default */
   uint32_t queue_capacity; /* wavefront: paths in flight, 0 = default */
-  uint32_t reserved;
+  uint32_t precision;      /* ZT_PRECISION_* */
 } zt_gpu_config;
 
 typedef struct zt_scene zt_scene;
@@ -124,6 +136,19 @@ zt_status zt_scene_build(zt_scene* scene);
  * *used_device (may be NULL) is 1 when the device built the BVH.
  * *build_ms (may be NULL) is the device time of the build. */
 zt_status zt_scene_build_device(zt_scene* scene, uint32_t* used_device, double* build_ms);
+
+/* Scene.build with the BVH the caller already built: the reference's
+ * Bvh.build output (bvh.zig:41-67; Node at bvh.zig:22-33, the shape
+ * permutation at bvh.zig:35-38), passed as n_nodes nodes and n_indices
+ * shape indices (n_indices = number of bounded shapes), used as given
+ * without rebuilding.  The emitter table is built as Scene.build does
+ * (light.zig:68-94).  The tree must be one the reference's build can
+ * produce in shape: root at 0, each interior node's two children adjacent at
+ * an odd index after it, every node reachable once, depth at most 64, leaves
+ * covering every shape position once, indices a permutation; anything else
+ * is ZT_ERR_INVALID_ARGUMENT and leaves the scene unbuilt. */
+zt_status zt_scene_set_bvh(zt_scene* scene, const zt_bvh_node* nodes, size_t n_nodes, const uint32_t* indices,
+                           size_t n_indices);
 
 /* ---- Inspection (Scene fields, Bvh, Lights) --------------------------- */
 zt_status zt_scene_counts(const zt_scene* scene, uint64_t* n_materials, uint64_t* n_bounded,

@@ -91,6 +91,9 @@ def lib() -> C.CDLL:
         _lib.ozt_scene_indices.argtypes = [C.c_void_p, C.c_void_p]
         _lib.ozt_scene_lights.argtypes = [C.c_void_p] * 4
         _lib.ozt_render.argtypes = [C.c_void_p] * 4
+        _lib.ozt_render_moments.argtypes = [C.c_void_p] * 4
+        _lib.ozt_render_pixels_moments.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                                   C.c_void_p]
         _lib.ozt_render_debug.argtypes = [C.c_void_p] * 4
         _lib.ozt_render_params.argtypes = [C.c_void_p] * 4
         _lib.ozt_lights_sample.argtypes = [C.c_void_p] * 7
@@ -234,6 +237,28 @@ class OracleScene:
         if stats:
             return img, dict(zip(STATS_FIELDS, list(st)))
         return img
+
+    def render_moments(self, width, height, spp, max_depth, threads=None, seed=0, light_sampling=True):
+        """The image and, per pixel, the mean squared sample luminance."""
+        threads = threads or os.cpu_count() or 1
+        o = self.options(width, height, spp, max_depth, threads, seed, 16, light_sampling)
+        out = np.zeros(width * height * 3)
+        m2 = np.zeros(width * height)
+        if lib().ozt_render_moments(self.h, _p(o), _p(out), _p(m2)) != 0:
+            raise ValueError("InvalidOptions")
+        return out.reshape(height * width, 3), m2
+
+    def render_pixels_moments(self, width, height, spp, max_depth, pixels, threads=None, seed=0,
+                              light_sampling=True):
+        """render_pixels plus each listed pixel's mean squared sample luminance."""
+        threads = threads or os.cpu_count() or 1
+        o = self.options(width, height, spp, max_depth, threads, seed, 16, light_sampling)
+        pix = np.ascontiguousarray(pixels, np.uint64)
+        out = np.zeros(len(pix) * 3)
+        m2 = np.zeros(len(pix))
+        if lib().ozt_render_pixels_moments(self.h, _p(o), _p(pix), len(pix), _p(out), _p(m2)) != 0:
+            raise ValueError("InvalidOptions")
+        return out.reshape(len(pix), 3), m2
 
     def render_pixels(self, width, height, spp, max_depth, pixels, threads=None, seed=0, light_sampling=True,
                       stats: bool = False):

@@ -969,6 +969,8 @@ typedef struct {
   /* pixel-subset mode */
   const uint64_t* pixels;
   size_t n_pixels;
+  /* optional: per pixel, the mean of the squared luminance of its samples */
+  double* moments;
 } octx;
 
 static void render_pixel(octx* c, uint64_t x, uint64_t y, double* dst, ostats* st) { /* render.zig:133-144 */
@@ -976,6 +978,7 @@ static void render_pixel(octx* c, uint64_t x, uint64_t y, double* dst, ostats* s
   const double inv_spp = 1.0 / (double)c->o->spp;
   orng rng = rng_for_stream(c->o->seed, y * c->o->width + x);
   ov3 sum = V(0, 0, 0);
+  double lum2 = 0;
   for (uint64_t i = 0; i < c->o->spp; ++i) {
     const double sx = ((double)x + rng_float(&rng)) / w;
     const double ty = ((double)y + rng_float(&rng)) / h;
@@ -983,12 +986,17 @@ static void render_pixel(octx* c, uint64_t x, uint64_t y, double* dst, ostats* s
     camera_ray(&c->cam, sx, ty, &rng, &ro, &rd);
     const ov3 col = trace_with(c->s, ro, rd, &rng, c->o->max_depth, (int)c->o->light_sampling, st, NULL, NULL);
     if (st) st->samples++;
-    if (visfinite(col)) sum = vadd(sum, col);
+    if (visfinite(col)) {
+      sum = vadd(sum, col);
+      const double lum = 0.2126 * col.x + 0.7152 * col.y + 0.0722 * col.z; /* light.zig:38-40 */
+      lum2 += lum * lum;
+    }
   }
   const ov3 px = vscale(sum, inv_spp);
   dst[0] = px.x;
   dst[1] = px.y;
   dst[2] = px.z;
+  if (c->moments) c->moments[(dst - c->out) / 3] = lum2 * inv_spp;
 }
 
 static void stats_add(ostats* a, const ostats* b) {
@@ -1064,6 +1072,45 @@ int ozt_render(const oscene* s, const ooptions* o, double* out, ostats* stats) {
   if (stats) memset(stats, 0, sizeof *stats);
   c.stats = stats;
   const int rc = run_render(&c);
+  pthread_mutex_destroy(&c.stats_lock);
+  return rc;
+}
+
+int ozt_render_moments(const oscene* s, const ooptions* o, double* out, double* moments) {
+  if (!options_valid(o)) return -1;
+  memset(out, 0, o->width * o->height * 3 * sizeof(double));
+  octx c;
+  memset(&c, 0, sizeof c);
+  c.s = s;
+  c.o = o;
+  c.out = out;
+  c.moments = moments;
+  camera_init(&s->camera, (double)o->width / (double)o->height, &c.cam);
+  c.tiles_x = (o->width + o->tile_size - 1) / o->tile_size;
+  c.tile_count = c.tiles_x * ((o->height + o->tile_size - 1) / o->tile_size);
+  atomic_init(&c.next_tile, 0);
+  pthread_mutex_init(&c.stats_lock, NULL);
+  const int rc = run_render(&c);
+  pthread_mutex_destroy(&c.stats_lock);
+  return rc;
+}
+
+int ozt_render_pixels_moments(const oscene* s, const ooptions* o, const uint64_t* pixels, size_t n, double* out,
+                              double* moments) {
+  if (!options_valid(o)) return -1;
+  octx c;
+  memset(&c, 0, sizeof c);
+  c.s = s;
+  c.o = o;
+  c.out = out;
+  c.moments = moments;
+  camera_init(&s->camera, (double)o->width / (double)o->height, &c.cam);
+  c.pixels = pixels;
+  c.n_pixels = n;
+  c.tile_count = (n + 63) / 64;
+  atomic_init(&c.next_tile, 0);
+  pthread_mutex_init(&c.stats_lock, NULL);
+  const int rc = c.tile_count ? run_render(&c) : 0;
   pthread_mutex_destroy(&c.stats_lock);
   return rc;
 }

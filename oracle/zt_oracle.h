@@ -97,6 +97,14 @@ int ozt_render_pixels(const oscene* s, const ooptions* o, const uint64_t* pixels
 /* First sample of every pixel: primitive id of the camera ray's closest hit
  * (-1 on a miss) and the number of extension rays the path traced. */
 int ozt_render_debug(const oscene* s, const ooptions* o, int32_t* first_prim, uint32_t* path_len);
+/* ozt_render plus, per pixel, the mean over its samples of the squared
+ * luminance (0.2126 r + 0.7152 g + 0.0722 b, light.zig:38-40) of each
+ * finite sample: the second-moment buffer behind the Monte Carlo standard
+ * error of an image's mean luminance. */
+int ozt_render_moments(const oscene* s, const ooptions* o, double* out_rgb, double* moments);
+/* The same for a list of pixels (as ozt_render_pixels). */
+int ozt_render_pixels_moments(const oscene* s, const ooptions* o, const uint64_t* pixels, size_t n,
+                              double* out_rgb, double* moments);
 
 /* The differentiable form's forward (detached sampling): the scene's
  * materials drive roulette, light pick and MIS weights, theta (3 per

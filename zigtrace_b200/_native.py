@@ -27,7 +27,7 @@ OPTIONS_DTYPE = np.dtype([("width", "<u8"), ("height", "<u8"), ("spp", "<u8"), (
 BVH_NODE_DTYPE = np.dtype([("bmin", "<f8", (3,)), ("bmax", "<f8", (3,)), ("first", "<u4"), ("count", "<u4")])
 LIGHT_DTYPE = np.dtype([("shape", SHAPE_DTYPE), ("radiance", "<f8", (3,)), ("weight", "<f8")])
 GPU_CONFIG_DTYPE = np.dtype([("mode", "<u4"), ("block_size", "<u4"), ("queue_capacity", "<u4"),
-                             ("reserved", "<u4")])
+                             ("precision", "<u4")])
 
 assert SHAPE_DTYPE.itemsize == 80 and MATERIAL_DTYPE.itemsize == 40
 assert CAMERA_DTYPE.itemsize == 104 and BACKGROUND_DTYPE.itemsize == 56
@@ -63,6 +63,7 @@ SIGNATURES = {
     "zt_scene_set_background": (_i32, [_P, _P]),
     "zt_scene_build": (_i32, [_P]),
     "zt_scene_build_device": (_i32, [_P, C.POINTER(_u32), C.POINTER(C.c_double)]),
+    "zt_scene_set_bvh": (_i32, [_P, _P, C.c_size_t, _P, C.c_size_t]),
     "zt_scene_counts": (_i32, [_P, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64),
                                C.POINTER(_u64)]),
     "zt_scene_bvh": (_i32, [_P, _P, _P]),

@@ -24,6 +24,7 @@ Vec = Sequence[float]
 LAMBERTIAN, METAL, DIELECTRIC, EMISSIVE = 0, 1, 2, 3
 SPHERE, TRIANGLE, PLANE = 0, 1, 2
 MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, MODE_MEGAKERNEL_REGEN = 0, 1, 2, 3
+PRECISION_EXACT, PRECISION_FAST = 0, 1
 
 
 # ---------------------------------------------------------------- Material --
@@ -155,14 +156,19 @@ class Options:
 
 @dataclass
 class GpuConfig:
-    """Device execution choices (zt_gpu_config); zeros mean defaults."""
+    """Device execution choices (zt_gpu_config); zeros mean defaults.
+    ``precision``: PRECISION_EXACT (bit-identical to the reference
+    algorithm) or PRECISION_FAST (single-precision conservative BVH boxes,
+    f64 everything else)."""
     mode: int = MODE_AUTO
     block_size: int = 0
     queue_capacity: int = 0
+    precision: int = 0
 
     def record(self) -> np.ndarray:
         r = np.zeros(1, N.GPU_CONFIG_DTYPE)
         r["mode"], r["block_size"], r["queue_capacity"] = self.mode, self.block_size, self.queue_capacity
+        r["precision"] = self.precision
         return r
 
 
@@ -279,6 +285,30 @@ class Scene:
             self.build_ms = ms.value if used.value else None
         else:
             N.check(lib.zt_scene_build(h))
+        return self
+
+    def build_with_bvh(self, nodes: np.ndarray, indices: np.ndarray) -> "Scene":
+        """Scene.build with a BVH built elsewhere -- the reference's own
+        ``Bvh.build`` output (``nodes`` in the zt_bvh_node layout, ``indices``
+        the shape permutation) -- used as given (zt_scene_set_bvh)."""
+        lib = N.lib()
+        self._invalidate()
+        h = C.c_void_p()
+        N.check(lib.zt_scene_create(C.byref(h)))
+        self._handle = h
+        mats = self.materials
+        if len(mats):
+            N.check(lib.zt_scene_add_materials(h, N.ptr(mats), len(mats), None))
+        shapes = self.shapes
+        if len(shapes):
+            N.check(lib.zt_scene_add_shapes(h, N.ptr(shapes), len(shapes)))
+        N.check(lib.zt_scene_set_camera(h, N.ptr(self.camera.record())))
+        N.check(lib.zt_scene_set_background(h, N.ptr(self.background.record())))
+        nodes = np.ascontiguousarray(nodes, N.BVH_NODE_DTYPE)
+        indices = np.ascontiguousarray(indices, np.uint32)
+        self.built_on_device, self.build_ms = False, None
+        N.check(lib.zt_scene_set_bvh(h, N.ptr(nodes) if len(nodes) else None, len(nodes),
+                                     N.ptr(indices) if len(indices) else None, len(indices)))
         return self
 
     @property

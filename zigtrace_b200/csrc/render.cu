@@ -33,7 +33,8 @@ using namespace zt;
 struct zt_host_staging {
   void* pinned = nullptr;
   size_t bytes = 0;
-  size_t off_prims = 0, off_ids = 0, off_pairs = 0, off_planes = 0, off_mats = 0, off_lights = 0, off_cdf = 0;
+  size_t off_prims = 0, off_ids = 0, off_pairs = 0, off_fpairs = 0, off_planes = 0, off_mats = 0, off_lights = 0,
+         off_cdf = 0;
   DevScene view;  /* counts, root, total; pointers unset */
 };
 
@@ -188,6 +189,7 @@ static zt_status make_staging(zt_scene* s) {
   stage(f.prims, cur, h->off_prims);
   stage(f.prim_ids, cur, h->off_ids);
   stage(f.pairs, cur, h->off_pairs);
+  stage(f.fpairs, cur, h->off_fpairs);
   stage(f.planes, cur, h->off_planes);
   stage(f.mats, cur, h->off_mats);
   stage(f.lights, cur, h->off_lights);
@@ -202,6 +204,7 @@ static zt_status make_staging(zt_scene* s) {
   stage_copy(f.prims, h->pinned, h->off_prims);
   stage_copy(f.prim_ids, h->pinned, h->off_ids);
   stage_copy(f.pairs, h->pinned, h->off_pairs);
+  stage_copy(f.fpairs, h->pinned, h->off_fpairs);
   stage_copy(f.planes, h->pinned, h->off_planes);
   stage_copy(f.mats, h->pinned, h->off_mats);
   stage_copy(f.lights, h->pinned, h->off_lights);
@@ -243,6 +246,7 @@ static zt_status upload(zt_scene* s) {
   d->view.prims = (const DPrim*)(b + h->off_prims);
   d->view.prim_ids = (const int32_t*)(b + h->off_ids);
   d->view.pairs = (const DPair*)(b + h->off_pairs);
+  d->view.fpairs = h->view.fast_ok ? (const FPair*)(b + h->off_fpairs) : nullptr;
   d->view.planes = (const DPrim*)(b + h->off_planes);
   d->view.mats = (const DMat*)(b + h->off_mats);
   d->view.lights = (const DLight*)(b + h->off_lights);
@@ -284,7 +288,7 @@ static RenderParams make_params(const zt_scene* s, const zt_options* o) {
 
 /* One pixel: renderTile's per-pixel body, render.zig:133-144.  kNee as for
  * trace_with. */
-template <bool kAux, bool kNee = true>
+template <bool kAux, bool kNee = true, bool kFast = false>
 __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderParams& p, uint64_t pix,
                                              double* __restrict__ out, TraceAux* aux) {
   const uint64_t x = pix % p.width, y = pix / p.width;
@@ -297,7 +301,7 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
     const double t = ((double)y + rng_float(rng)) / h;
     dv3 ro, rd;
     camera_ray(p.cam, s, t, rng, ro, rd);
-    const dv3 c = trace_with<kAux, kNee>(sc, ro, rd, rng, p.max_depth, p.use_nee != 0, aux);
+    const dv3 c = trace_with<kAux, kNee, kFast>(sc, ro, rd, rng, p.max_depth, p.use_nee != 0, aux);
     if (kAux) break;
     if (visfinite(c)) sum = sum + c;
   }
@@ -320,7 +324,7 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
 constexpr int kMegaThreadsPerSm = 896;
 constexpr int kMegaThreadsPerSmNoNee = 896;
 
-template <int BS, bool kNee>
+template <int BS, bool kNee, bool kFast = false>
 __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
     k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out, unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
@@ -332,7 +336,7 @@ __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPe
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) return;
     const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
-    if (x < p.width && y < row_end) render_pixel<false, kNee>(sc, p, y * p.width + x, out, nullptr);
+    if (x < p.width && y < row_end) render_pixel<false, kNee, kFast>(sc, p, y * p.width + x, out, nullptr);
   }
 }
 
@@ -345,6 +349,7 @@ __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPe
  * valid = false).  Pays off when path lengths vary widely within a warp
  * (closed scenes such as the Cornell box); on open scenes with short paths
  * the nested form is faster. */
+template <bool kFast>
 __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const RenderParams& p, uint64_t x, uint64_t y,
                                                    bool valid, double* __restrict__ out) {
   const double w = (double)p.width, h = (double)p.height;
@@ -377,7 +382,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
     bool end = depth >= p.max_depth;
     if (!end) {
       Hit hit;
-      if (!scene_intersect<false>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
+      if (!scene_intersect<false, kFast>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
         radiance = radiance + vmul(throughput, background_radiance(sc.bg, rd));
         end = true;
       } else {
@@ -388,7 +393,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
           radiance = radiance + vscale(vmul(throughput, le), wt);
         }
         if (mat.kind == kLambertian && use_nee)
-          radiance = radiance + vmul(throughput, direct_light(sc, L3(mat.color), hit, rng));
+          radiance = radiance + vmul(throughput, direct_light<kFast>(sc, L3(mat.color), hit, rng));
         dv3 atten, sd;
         if (!material_scatter(mat, rd, hit, rng, atten, sd)) {
           end = true;
@@ -427,7 +432,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
  * per SM (up to 128 registers, no spills): 1.17x the seven-block build on the
  * Cornell box, whose 65,536 pixels fill only a quarter of the GPU's thread
  * slots anyway, and equal to it on 1280x720 random spheres. */
-template <int BS>
+template <int BS, bool kFast = false>
 __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
                                                              unsigned int* __restrict__ counter) {
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, Rend
     tile = __shfl_sync(0xffffffffu, tile, 0);
     if ((uint64_t)tile >= tiles) return;
     const uint64_t x = (tile % tiles_x) * 8 + (lane & 7), y = p.row0 + (tile / tiles_x) * 4 + (lane >> 3);
-    render_pixel_regen(sc, p, x, y, x < p.width && y < row_end, out);
+    render_pixel_regen<kFast>(sc, p, x, y, x < p.width && y < row_end, out);
   }
 }
 
@@ -459,7 +464,7 @@ struct BatchItem {
  * render them with the item's own scene and parameters, so small images do
  * not leave the GPU idle the way one launch per image does.  kNee = false
  * is the instance for batches in which no render samples lights. */
-template <int BS, bool kNee>
+template <int BS, bool kNee, bool kFast = false>
 __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
     k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
                    unsigned int* __restrict__ counter) {
@@ -479,7 +484,7 @@ __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPe
     const uint64_t local = tile - it.tile_begin;
     const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
     if (x < it.p.width && y < it.p.height)
-      render_pixel<false, kNee>(it.sc, it.p, y * it.p.width + x, it.out, nullptr);
+      render_pixel<false, kNee, kFast>(it.sc, it.p, y * it.p.width + x, it.out, nullptr);
   }
 }
 
@@ -712,30 +717,51 @@ static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
 enum MegaVariant { kMegaNested = 0, kMegaRegen = 1 };
 constexpr double kRegenMeanPath = 3.0;
 
-template <int BS>
-static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
-                           MegaVariant variant, cudaStream_t stream) {
+template <int BS, bool kFast>
+static void launch_mega_bsf(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
+                            MegaVariant variant, cudaStream_t stream) {
   const uint64_t npix = p.width * p.rows;
   if (variant == kMegaRegen)
-    k_render_regen<BS><<<persistent_grid(k_render_regen<BS>, BS, npix), BS, 0, stream>>>(v, p, d_out, counter);
-  else if (p.use_nee)
-    k_render_mega<BS, true><<<persistent_grid(k_render_mega<BS, true>, BS, npix), BS, 0, stream>>>(v, p, d_out,
-                                                                                                    counter);
-  else
-    k_render_mega<BS, false><<<persistent_grid(k_render_mega<BS, false>, BS, npix), BS, 0, stream>>>(v, p, d_out,
+    k_render_regen<BS, kFast><<<persistent_grid(k_render_regen<BS, kFast>, BS, npix), BS, 0, stream>>>(v, p, d_out,
                                                                                                       counter);
+  else if (p.use_nee)
+    k_render_mega<BS, true, kFast><<<persistent_grid(k_render_mega<BS, true, kFast>, BS, npix), BS, 0, stream>>>(
+        v, p, d_out, counter);
+  else
+    k_render_mega<BS, false, kFast><<<persistent_grid(k_render_mega<BS, false, kFast>, BS, npix), BS, 0, stream>>>(
+        v, p, d_out, counter);
+}
+
+template <int BS>
+static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
+                           MegaVariant variant, bool fast, cudaStream_t stream) {
+  if (fast) launch_mega_bsf<BS, true>(v, p, d_out, counter, variant, stream);
+  else launch_mega_bsf<BS, false>(v, p, d_out, counter, variant, stream);
 }
 
 static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
 
+/* Whether a render takes the fast traversal: asked for, and the scene has
+ * its float records (a scene whose leaves or bounds do not fit them renders
+ * with the f64 traversal).  The camera origin must be within the records'
+ * coordinate range as well. */
+static bool use_fast(const zt_scene* s, const RenderParams& p, uint32_t precision) {
+  if (precision != ZT_PRECISION_FAST || !s->device || !s->device->view.fast_ok) return false;
+  const double* o = p.cam.origin;
+  const double reach = fabs(p.cam.lens_radius) * (fabs(p.cam.u[0]) + fabs(p.cam.u[1]) + fabs(p.cam.u[2]) +
+                                                  fabs(p.cam.v[0]) + fabs(p.cam.v[1]) + fabs(p.cam.v[2]));
+  return fabs(o[0]) + reach <= kFastMaxCoord && fabs(o[1]) + reach <= kFastMaxCoord &&
+         fabs(o[2]) + reach <= kFastMaxCoord;
+}
+
 static zt_status launch_mega(zt_scene* s, const RenderParams& p, uint32_t block_size, double* d_out,
-                             MegaVariant variant, cudaStream_t stream) {
+                             MegaVariant variant, bool fast, cudaStream_t stream) {
   zt_device_buffers* d = s->device;
   ZT_CUDA(cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream), "reset work counter");
   const DevScene v = launch_view(s);
-  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, variant, stream);
-  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, variant, stream);
-  else launch_mega_bs<128>(v, p, d_out, d->counter, variant, stream);
+  if (block_size == 64) launch_mega_bs<64>(v, p, d_out, d->counter, variant, fast, stream);
+  else if (block_size == 256) launch_mega_bs<256>(v, p, d_out, d->counter, variant, fast, stream);
+  else launch_mega_bs<128>(v, p, d_out, d->counter, variant, fast, stream);
   ZT_CUDA(cudaGetLastError(), "launch the megakernel");
   return ZT_OK;
 }
@@ -866,10 +892,12 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
+  const uint32_t precision = cfg ? cfg->precision : ZT_PRECISION_EXACT;
+  if (precision > ZT_PRECISION_FAST) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.precision");
   const bool long_paths = s->pilot_valid && s->mean_path >= kRegenMeanPath;
   const MegaVariant variant =
       (mode == ZT_MODE_MEGAKERNEL_REGEN || (mode == ZT_MODE_AUTO && long_paths)) ? kMegaRegen : kMegaNested;
-  return launch_mega(s, p, bs, d_out, variant, stream);
+  return launch_mega(s, p, bs, d_out, variant, use_fast(s, p, precision), stream);
 }
 
 /* Error word of the last wavefront launch (after the stream is idle). */
@@ -1016,7 +1044,8 @@ zt_status zt_render_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, u
   }
   double* d_out = nullptr;
   if ((rc = pool_alloc((void**)&d_out, bytes, 0, "allocate framebuffer band")) != ZT_OK) return rc;
-  rc = launch_mega(s, p, 0, d_out, s->pilot_valid && s->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested, 0);
+  rc = launch_mega(s, p, 0, d_out, s->pilot_valid && s->mean_path >= kRegenMeanPath ? kMegaRegen : kMegaNested,
+                   false, 0);
   if (rc == ZT_OK) {
     cudaError_t e = cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
@@ -1435,6 +1464,7 @@ struct zt_batch {
   uint64_t total_tiles = 0;
   uint32_t block_size = 128;
   bool nee = true; /* some render of the batch samples lights */
+  bool fast = false; /* every render takes the fast traversal */
   BatchItem* d_items = nullptr;
   unsigned int* d_counter = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1442,16 +1472,22 @@ struct zt_batch {
 
 namespace zt {
 
-template <int BS, bool kNee>
+template <int BS, bool kNee, bool kFast>
 static void launch_batch_kernel(const zt_batch* b, cudaStream_t st) {
-  k_render_batch<BS, kNee><<<persistent_grid(k_render_batch<BS, kNee>, BS, b->total_tiles * 32), BS, 0, st>>>(
-      b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
+  k_render_batch<BS, kNee, kFast>
+      <<<persistent_grid(k_render_batch<BS, kNee, kFast>, BS, b->total_tiles * 32), BS, 0, st>>>(
+          b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
 }
 
 template <int BS>
 static void launch_batch_bs(const zt_batch* b, cudaStream_t st) {
-  if (b->nee) launch_batch_kernel<BS, true>(b, st);
-  else launch_batch_kernel<BS, false>(b, st);
+  if (b->fast) {
+    if (b->nee) launch_batch_kernel<BS, true, true>(b, st);
+    else launch_batch_kernel<BS, false, true>(b, st);
+  } else {
+    if (b->nee) launch_batch_kernel<BS, true, false>(b, st);
+    else launch_batch_kernel<BS, false, false>(b, st);
+  }
 }
 
 static void batch_free(zt_batch* b) {
@@ -1511,6 +1547,13 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
   b->block_size = bs ? bs : 128;
   b->nee = false;
   for (uint64_t k = 0; k < n; ++k) b->nee = b->nee || items[k].p.use_nee != 0;
+  const uint32_t precision = cfg ? cfg->precision : ZT_PRECISION_EXACT;
+  if (precision > ZT_PRECISION_FAST) {
+    delete b;
+    return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.precision");
+  }
+  b->fast = precision == ZT_PRECISION_FAST;
+  for (uint64_t k = 0; k < n && b->fast; ++k) b->fast = use_fast(scenes[idx[k]], items[k].p, precision);
   cudaError_t e = cudaGetDevice(&b->device);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_items, n * sizeof(BatchItem));
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(unsigned int));

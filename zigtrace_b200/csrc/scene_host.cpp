@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <new>
 
 namespace zt {
@@ -286,6 +287,88 @@ zt_status build_scene(zt_scene* s, bool device, bool* used_device, double* build
   return rc;
 }
 
+/* Scene.build with a BVH built elsewhere (the reference's own Bvh.build,
+ * bvh.zig:41-67, for a caller that already holds it): the tree is checked
+ * to be one this renderer can traverse exactly as the reference does, then
+ * used as given; the emitter table is built as Scene.build builds it
+ * (light.zig:68-94).  The checks: indices is a permutation of the bounded
+ * shapes; node 0 is the root; an interior node's children sit at first and
+ * first + 1 with first odd (the reference appends children in pairs after
+ * the root, so every pair of siblings starts at an odd index); every node
+ * but the root is the child of exactly one node; no node is deeper than
+ * the reference's max_depth (64), so the traversal stack of max_depth + 2
+ * entries (bvh.zig:87) cannot overflow; leaves cover [0, n) exactly once. */
+zt_status import_bvh(zt_scene* s, const zt_bvh_node* nodes, size_t n_nodes, const uint32_t* indices, size_t n_idx) {
+  for (const zt_shape& sh : s->shapes)
+    if (sh.material >= s->materials.size()) return fail(ZT_ERR_INVALID_ARGUMENT, "shape refers to an undefined material");
+  for (const zt_shape& sh : s->planes)
+    if (sh.material >= s->materials.size()) return fail(ZT_ERR_INVALID_ARGUMENT, "plane refers to an undefined material");
+  const size_t n = s->shapes.size();
+  auto bad = [](const std::string& why) { return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_set_bvh: " + why); };
+  if (n > 0xFFFFFFFFull / 2) return fail(ZT_ERR_TOO_MANY_PRIMITIVES, "TooManyPrimitives"); /* bvh.zig:44 */
+  if (n_idx != n) return bad("indices must hold one entry per bounded shape");
+  if (n == 0) {
+    if (n_nodes != 0) return bad("a scene without bounded shapes has no nodes");
+  } else {
+    if (!nodes || !indices) return bad("NULL nodes or indices");
+    if (n_nodes == 0 || n_nodes > 2 * n - 1 || n_nodes % 2 == 0)
+      return bad("node count must be odd and between 1 and 2n-1");
+  }
+  std::vector<uint8_t> seen(n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    if (indices[i] >= n || seen[indices[i]]) return bad("indices is not a permutation of the bounded shapes");
+    seen[indices[i]] = 1;
+  }
+  std::vector<uint8_t> level(n_nodes, 0), reached(n_nodes, 0);
+  std::vector<uint8_t> covered(n, 0);
+  if (n_nodes) reached[0] = 1;
+  /* children always follow their parent (first is odd and > parent), so one
+   * pass in index order visits every parent before its children */
+  for (size_t i = 0; i < n_nodes; ++i) {
+    if (!reached[i]) return bad("node " + std::to_string(i) + " is not reachable from the root");
+    const zt_bvh_node& nd = nodes[i];
+    if (nd.count == 0) {
+      const uint64_t l = nd.first;
+      if (l % 2 == 0 || l <= i || l + 1 >= n_nodes)
+        return bad("interior node " + std::to_string(i) + " has children outside the node array or not in a pair");
+      if (level[i] >= kMaxDepth) return bad("tree deeper than 64 levels");
+      for (uint64_t c = l; c <= l + 1; ++c) {
+        if (reached[c]) return bad("node " + std::to_string(c) + " has two parents");
+        reached[c] = 1;
+        level[c] = level[i] + 1;
+      }
+    } else {
+      if ((uint64_t)nd.first + nd.count > n) return bad("leaf " + std::to_string(i) + " reaches past the last shape");
+      for (uint64_t k = nd.first; k < (uint64_t)nd.first + nd.count; ++k) {
+        if (covered[k]) return bad("two leaves share shape position " + std::to_string(k));
+        covered[k] = 1;
+      }
+    }
+  }
+  for (size_t k = 0; k < n; ++k)
+    if (!covered[k]) return bad("shape position " + std::to_string(k) + " is in no leaf");
+  release_staging(s);
+  s->built = false;
+  s->pilot_valid = false;
+  try {
+    s->nodes.resize(n_nodes);
+    for (size_t i = 0; i < n_nodes; ++i) {
+      HostNode& h = s->nodes[i];
+      h.bmin[0] = nodes[i].bmin.x; h.bmin[1] = nodes[i].bmin.y; h.bmin[2] = nodes[i].bmin.z;
+      h.bmax[0] = nodes[i].bmax.x; h.bmax[1] = nodes[i].bmax.y; h.bmax[2] = nodes[i].bmax.z;
+      h.first = nodes[i].first;
+      h.count = nodes[i].count;
+    }
+    s->indices.assign(indices, indices + n);
+    const zt_status rc = build_lights(s);
+    if (rc != ZT_OK) return rc;
+  } catch (const std::bad_alloc&) {
+    return fail(ZT_ERR_OUT_OF_MEMORY, "OutOfMemory in zt_scene_set_bvh");
+  }
+  s->built = true;
+  return ZT_OK;
+}
+
 /* ---------------------------------------------------------- Camera ---- */
 static inline void v3_sub(const zt_vec3& a, const zt_vec3& b, double o[3]) {
   o[0] = a.x - b.x; o[1] = a.y - b.y; o[2] = a.z - b.z;
@@ -351,6 +434,66 @@ static DPrim to_prim(const zt_shape& s) {
   return p;
 }
 
+/* Nearest float at or below / at or above x. */
+static float f32_down(double x) {
+  float f = (float)x;
+  if ((double)f > x) f = std::nextafterf(f, -INFINITY);
+  return f;
+}
+static float f32_up(double x) {
+  float f = (float)x;
+  if ((double)f < x) f = std::nextafterf(f, INFINITY);
+  return f;
+}
+
+/* The fast traversal's float records (zt_types.h FPair): every box of the
+ * f64 tree moved outward by eps[axis] = 2^-20 * M[axis], M the largest
+ * |bound| of the root box on that axis, then rounded outward.  The margin
+ * covers the float slab test's rounding of box coordinates (the error
+ * analysis is in zt_fast.cuh), so a ray whose f64 slab test reaches a box
+ * also reaches its float copy.  Left empty (fast traversal unavailable) when
+ * a leaf holds more than kFastMaxLeaf primitives, the tree is too large for
+ * the packed payload word, or the bounds exceed kFastMaxCoord. */
+static void make_fast_records(const zt_scene* s, FlatScene* f) {
+  DevScene& v = f->view;
+  v.fast_ok = 0;
+  f->fpairs.clear();
+  const size_t nn = s->nodes.size();
+  if (nn == 0 || s->shapes.size() > kFastFirstMask || f->pairs.size() > kFastFirstMask) return;
+  double eps[3];
+  for (int k = 0; k < 3; ++k) {
+    const double m = std::max(std::fabs(s->nodes[0].bmin[k]), std::fabs(s->nodes[0].bmax[k]));
+    if (!(m <= kFastMaxCoord)) return; /* also rejects NaN */
+    eps[k] = std::ldexp(m, -20);
+  }
+  for (const HostNode& nd : s->nodes)
+    if (nd.count > kFastMaxLeaf) return;
+  auto word = [&](uint32_t c) -> uint32_t {
+    const HostNode& nd = s->nodes[c];
+    return nd.count > 0 ? (nd.count << kFastCountShift) | nd.first : (nd.first - 1) / 2;
+  };
+  f->fpairs.assign(f->pairs.size(), FPair{});
+  for (size_t i = 0; i < nn; ++i) {
+    const HostNode& nd = s->nodes[i];
+    if (nd.count > 0) continue;
+    FPair& pr = f->fpairs[(nd.first - 1) / 2];
+    for (int c = 0; c < 2; ++c) {
+      const HostNode& ch = s->nodes[nd.first + c];
+      for (int k = 0; k < 3; ++k) {
+        pr.lo[c][k] = f32_down(ch.bmin[k] - eps[k]);
+        pr.hi[c][k] = f32_up(ch.bmax[k] + eps[k]);
+      }
+      pr.word[c] = word(nd.first + c);
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    v.froot_lo[k] = f32_down(s->nodes[0].bmin[k] - eps[k]);
+    v.froot_hi[k] = f32_up(s->nodes[0].bmax[k] + eps[k]);
+  }
+  v.froot_word = word(0);
+  v.fast_ok = 1;
+}
+
 void flatten_scene(const zt_scene* s, FlatScene* f) {
   const size_t n = s->shapes.size();
   f->prims.resize(n);
@@ -383,6 +526,7 @@ void flatten_scene(const zt_scene* s, FlatScene* f) {
     for (int k = 0; k < 3; ++k) { v.root_lo[k] = s->nodes[0].bmin[k]; v.root_hi[k] = s->nodes[0].bmax[k]; }
     payload(0, v.root_first, v.root_count);
   }
+  make_fast_records(s, f);
   f->planes.resize(s->planes.size());
   for (size_t i = 0; i < s->planes.size(); ++i) f->planes[i] = to_prim(s->planes[i]);
   f->mats.resize(s->materials.size());
@@ -528,6 +672,12 @@ zt_status zt_scene_set_background(zt_scene* s, const zt_background* bg) {
   if (memcmp(&s->background, bg, sizeof *bg) != 0) s->pilot_valid = false;
   s->background = *bg;
   return ZT_OK;
+}
+
+zt_status zt_scene_set_bvh(zt_scene* s, const zt_bvh_node* nodes, size_t n_nodes, const uint32_t* indices,
+                           size_t n_indices) {
+  if (!s) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_scene_set_bvh: NULL scene");
+  return import_bvh(s, nodes, n_nodes, indices, n_indices);
 }
 
 zt_status zt_scene_build(zt_scene* s) {

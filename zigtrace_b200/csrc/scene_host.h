@@ -33,6 +33,7 @@ struct FlatScene {
   std::vector<DPrim> prims;
   std::vector<int32_t> prim_ids;
   std::vector<DPair> pairs;
+  std::vector<FPair> fpairs; /* conservative float copy of pairs (empty when the fast traversal cannot be used) */
   std::vector<DPrim> planes;
   std::vector<DMat> mats;
   std::vector<DLight> lights;

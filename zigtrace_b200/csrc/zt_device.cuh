@@ -263,15 +263,7 @@ ZT_D void hit_from(const DevScene& sc, int32_t k, dv3 o, dv3 d, double t, Hit& o
   }
 }
 
-template <bool kAnyHit>
-ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, Hit& out) {
-  double t;
-  const int32_t k = scene_query<kAnyHit>(sc, o, d, tmin, tmax, t);
-  if (k == -1) return false;
-  out.t = t;
-  if (!kAnyHit) hit_from(sc, k, o, d, t, out);
-  return true;
-}
+
 
 /* Returns the prim code of the closest hit (>= 0: prims[k]; <= -2:
  * planes[-2 - k]; -1: no hit) and its distance.  any_hit is a run-time flag
@@ -415,6 +407,25 @@ ZT_D bool scene_occluded(const DevScene& sc, dv3 o, dv3 d, double tmin, double t
     if (prim_t(sc.planes[i], o, d, tmin, tmax, th)) return true;
   }
   return false;
+}
+
+}  // namespace zt
+
+#include "zt_fast.cuh"
+
+namespace zt {
+
+/* Closest or any hit with the hit record (kAnyHit: t only).  kFast walks
+ * the float records (zt_fast.cuh) for closest-hit queries. */
+template <bool kAnyHit, bool kFast = false>
+ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, Hit& out) {
+  double t;
+  const int32_t k = (kFast && !kAnyHit) ? scene_query_fast(sc, o, d, tmin, tmax, t)
+                                        : scene_query<kAnyHit>(sc, o, d, tmin, tmax, t);
+  if (k == -1) return false;
+  out.t = t;
+  if (!kAnyHit) hit_from(sc, k, o, d, t, out);
+  return true;
 }
 
 /* ---------------------------------------------------------- Material ---- */
@@ -587,14 +598,19 @@ ZT_D double power_weight(double a, double b) { /* render.zig:38-41 */
   return a2 / (a2 + b * b);
 }
 
-/* directLight, render.zig:46-56 (shadow ray as an any-hit query). */
+/* directLight, render.zig:46-56 (shadow ray as an any-hit query; kFast
+ * walks the float records). */
+template <bool kFast = false>
 ZT_D dv3 direct_light(const DevScene& sc, dv3 albedo, const Hit& hit, Rng& rng) {
   dv3 ldir, lrad;
   double ldist, lpdf;
   if (!lights_sample(sc, hit.point, rng, ldir, ldist, lrad, lpdf)) return V(0, 0, 0);
   const double cos_s = vdot(hit.normal, ldir);
   if (cos_s <= 0 || !(lpdf > 0)) return V(0, 0, 0);
-  if (scene_occluded(sc, hit.point, ldir, kRayEpsilon, ldist * (1 - 1e-6))) return V(0, 0, 0);
+  const double shadow_tmax = ldist * (1 - 1e-6);
+  if (kFast ? scene_occluded_fast(sc, hit.point, ldir, kRayEpsilon, shadow_tmax)
+            : scene_occluded(sc, hit.point, ldir, kRayEpsilon, shadow_tmax))
+    return V(0, 0, 0);
   const double bsdf_pdf = cos_s / kPi;
   const double scale = cos_s / (kPi * lpdf) * power_weight(lpdf, bsdf_pdf);
   return vscale(vmul(albedo, lrad), scale);
@@ -605,7 +621,7 @@ ZT_D dv3 direct_light(const DevScene& sc, dv3 albedo, const Hit& hit, Rng& rng) 
  * path is then the reference's use_nee = false path, draw for draw. */
 struct TraceAux { int32_t first_prim; uint32_t path_len; };
 
-template <bool kAux, bool kNee = true>
+template <bool kAux, bool kNee = true, bool kFast = false>
 ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_depth, bool use_nee_arg,
                     TraceAux* aux) {
   const bool use_nee = kNee && use_nee_arg;
@@ -617,7 +633,7 @@ ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_d
   for (uint64_t depth = 0; depth < max_depth; ++depth) {
     Hit hit;
     if (kAux) n_ext++;
-    if (!scene_intersect<false>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
+    if (!scene_intersect<false, kFast>(sc, ro, rd, kRayEpsilon, INFINITY, hit)) {
       if (kAux) aux->path_len = n_ext;
       return radiance + vmul(throughput, background_radiance(sc.bg, rd));
     }
@@ -630,7 +646,7 @@ ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_d
       radiance = radiance + vscale(vmul(throughput, le), w);
     }
     if (mat.kind == kLambertian && use_nee)
-      radiance = radiance + vmul(throughput, direct_light(sc, L3(mat.color), hit, rng));
+      radiance = radiance + vmul(throughput, direct_light<kFast>(sc, L3(mat.color), hit, rng));
     dv3 atten, sd;
     if (!material_scatter(mat, rd, hit, rng, atten, sd)) break;
     throughput = vmul(throughput, atten);

@@ -52,6 +52,26 @@ struct ZT_ALIGN(128) DPair {
   uint32_t count[2];
 };
 
+/* 64 bytes: the same two children as a DPair, for the fast traversal
+ * (zt_fast.cuh).  Boxes are single precision and conservative: every bound
+ * is moved outward by eps[axis] = 2^-20 * max(|root lo|, |root hi|) on that
+ * axis and then rounded outward to float, so the box contains the f64 box
+ * with a margin that covers the float slab test's rounding.  word[c] packs
+ * the child's payload: count << 28 | first (count 0: first is the record of
+ * the child's own children). */
+struct ZT_ALIGN(64) FPair {
+  float lo[2][3];
+  float hi[2][3];
+  uint32_t word[2];
+  uint32_t pad[2];
+};
+constexpr uint32_t kFastCountShift = 28;
+constexpr uint32_t kFastFirstMask = (1u << kFastCountShift) - 1;
+constexpr uint32_t kFastMaxLeaf = (1u << (32 - kFastCountShift)) - 1;
+/* Largest |coordinate| (of the scene's bounds and of ray origins) the float
+ * slab test handles: products with the clamped reciprocal stay finite. */
+constexpr double kFastMaxCoord = 1e7;
+
 struct ZT_ALIGN(16) DMat {
   double color[3];
   double param;
@@ -100,6 +120,11 @@ struct DevScene {
   uint32_t pad;
   double total;       /* Lights.total */
   DBackground bg;
+  /* fast traversal (zt_fast.cuh): conservative float records and root box */
+  const FPair* fpairs;
+  float froot_lo[3], froot_hi[3];
+  uint32_t froot_word;
+  uint32_t fast_ok;   /* 1 when the fast records exist (leaves <= 15 primitives, bounds within kFastMaxCoord) */
 };
 
 struct RenderParams {

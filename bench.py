@@ -90,6 +90,9 @@ def parse_args():
                    help="default workload only: skip the batch and diff sub-objects")
     p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
     p.add_argument("--capacity", type=int, default=0, help="zt_gpu_config.queue_capacity (wavefront)")
+    p.add_argument("--shard", choices=["frames", "rows"], default="frames",
+                   help="frames: one frame per rank (weak scaling); rows: one frame split into row bands across "
+                        "ranks and all-gathered on the device (strong scaling)")
     p.add_argument("--precision", choices=["exact", "fast"], default="fast",
                    help="zt_gpu_config.precision of the measured render (exact = the verification build)")
     return p.parse_args()
@@ -271,8 +274,11 @@ def b200_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local_rank)
-    if world > 1:
+    if world > 1 or args.shard == "rows":
         from datetime import timedelta
+        if "MASTER_ADDR" not in os.environ:  # a single-rank group for the row-sharded mode at N=1
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(29500 + os.getpid() % 1000), RANK="0",
+                              WORLD_SIZE="1")
         dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local_rank))
 
     def barrier():
@@ -286,6 +292,12 @@ def b200_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.shard == "rows":
+        line = shard_rows_arm(args, world, rank, local_rank, barrier, allmax)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.destroy_process_group()
+        return
     if args.workload in ("batch", "diff"):
         arm = batch_arm if args.workload == "batch" else diff_arm
         line = arm(args, world, rank, local_rank, barrier, allmax)
@@ -450,6 +462,82 @@ def b200_arm(args):
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def shard_rows_arm(args, world, rank, local_rank, barrier, allmax):
+    """One frame of the workload split into row bands across the ranks: each
+    rank renders its band into its slot of a device buffer
+    (zt_render_rows_device) and one NCCL all-gather assembles the frame on
+    every rank, inside the timed region.  value = the frame's samples over
+    the max-over-ranks time per frame (strong scaling: the frame is fixed)."""
+    import torch
+    import torch.distributed as dist
+
+    import zigtrace_b200 as zt
+    from zigtrace_b200 import sharding
+
+    scene, o = workload(args.workload, args.spp)
+    scene.build(device=True)
+    scene.upload()
+    prec = zt.PRECISION_FAST if args.precision == "fast" else zt.PRECISION_EXACT
+    gcfg = zt.GpuConfig(mode=args.mode, precision=prec)
+    height, width = int(o.height), int(o.width)
+    bands = sharding.row_bands(height, world)
+    y0, y1 = bands[rank]
+    max_rows = max(b - a for a, b in bands)
+    buf = torch.zeros(max_rows * width * 3, dtype=torch.float64, device="cuda")
+    gathered = torch.empty(world * buf.numel(), dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        zt.render_rows_device(scene, o, y0, y1, buf.data_ptr(), stream.cuda_stream, gcfg)
+        dist.all_gather_into_tensor(gathered, buf)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    a.record(stream)
+    for i in range(args.steps):
+        flush.zero_()
+        k0[i].record(stream)
+        step()
+        k1[i].record(stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = allmax(a.elapsed_time(b)) / args.steps
+    frame_ms = allmax(statistics.mean(k0[i].elapsed_time(k1[i]) for i in range(args.steps)))
+    samples = width * height * o.spp
+    stride = buf.numel()
+    img = torch.cat([gathered[r * stride:r * stride + (q - p) * width * 3] for r, (p, q) in enumerate(bands)])
+    whole = torch.empty(width * height * 3, dtype=torch.float64, device="cuda")
+    zt.render_device(scene, o, whole.data_ptr(), stream.cuda_stream, gcfg)
+    torch.cuda.synchronize()
+    identical = bool(torch.equal(img, whole))
+    counts = scene.counts()
+    return {
+        "metric": "Msamples/s", "value": round(samples / (ms / 1e3) / 1e6, 4), "unit": "Msamples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded procedural scene)",
+        "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
+                   "precision": args.precision,
+                   "sharding": f"one frame in {world} row bands (rows {bands}), band rendered into its slot of "
+                               "the gather buffer, one NCCL all-gather per frame inside the timed region"},
+        "frame_ms_with_gather": round(frame_ms, 3), "gathered_equals_single_device_render": identical,
+        "gpu_launches": args.steps, "clocks": clk, "roofline": None, "cpu_baseline": None,
+        "e2e": None,
+    }
 
 
 def batch_arm(args, world, rank, local_rank, barrier, allmax):

@@ -187,6 +187,16 @@ zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_con
  * must have been uploaded to the current device. */
 zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                            double* d_out_rgb, void* stream);
+/* Device-resident band: rows [row_begin, row_end) of the width x height
+ * image (the same camera and per-pixel RNG streams, so the band equals those
+ * rows of the whole image) into the device buffer d_out_rgb of
+ * (row_end - row_begin)*width*3 doubles, enqueued on `stream` without
+ * synchronising.  One rank's share of a frame sharded across GPUs, written
+ * straight into its slot of a collective's buffer.  Megakernel modes only
+ * (ZT_MODE_WAVEFRONT is rejected); cfg may be NULL.  The scene must have been
+ * uploaded to the current device. */
+zt_status zt_render_rows_device(zt_scene* scene, const zt_options* opts, uint64_t row_begin, uint64_t row_end,
+                                const zt_gpu_config* cfg, double* d_out_rgb, void* stream);
 /* ---- Differentiable form ------------------------------------------------ */
 /* Gradients of an image loss with respect to every material's colour (the
  * albedo of Lambertian and metal materials, the radiance of emissive ones;

@@ -171,10 +171,35 @@ def test_render_sharded_over_nccl_single_rank():
     try:
         scene = scenes.cornell().build()
         o = zt.Options(64, 40, 2, 16)
-        img = sharding.render_sharded(scene, o)
+        scene.upload()
+        img = sharding.render_sharded(scene, o)  # band rendered into the gather buffer on the device
         assert img.tobytes() == zt.render(scene, o).pixels.tobytes()
+        dev = sharding.render_sharded(scene, o, as_numpy=False)
+        assert dev.is_cuda and dev.cpu().numpy().tobytes() == img.tobytes()
+        fast = sharding.render_sharded(scene, o, gpu=zt.GpuConfig(precision=zt.PRECISION_FAST))
+        assert (fast == img).all(axis=1).mean() > 0.99  # the fast walk: nearly every pixel identical
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", [zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN])
+def test_device_row_bands_reassemble_the_image(mode):
+    import torch
+    scene = scenes.random_spheres().build()
+    scene.upload()
+    o = zt.Options(200, 113, 3, 50, seed=4)
+    full = zt.render(scene, o).pixels
+    bands = [(0, 1), (1, 40), (40, 113)]
+    out = torch.full((o.width * o.height * 3,), -1.0, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for a, b in bands:
+        zt.render_rows_device(scene, o, a, b, out.data_ptr() + 8 * a * o.width * 3, st, zt.GpuConfig(mode))
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().reshape(-1, 3).tobytes() == full.tobytes()
+    with pytest.raises(zt.ZigtraceError):
+        zt.render_rows_device(scene, o, 50, 40, out.data_ptr(), st)
+    with pytest.raises(zt.ZigtraceError):
+        zt.render_rows_device(scene, o, 0, 10, out.data_ptr(), st, zt.GpuConfig(zt.MODE_WAVEFRONT))
 
 
 @pytest.mark.parametrize("mode", MODES)

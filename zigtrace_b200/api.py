@@ -492,6 +492,17 @@ def render_device(scene: Scene, opts: Options, d_out_ptr: int, stream_ptr: int,
                                      C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr)))
 
 
+def render_rows_device(scene: Scene, opts: Options, y0: int, y1: int, d_out_ptr: int, stream_ptr: int = 0,
+                       gpu: Optional[GpuConfig] = None) -> None:
+    """Enqueues rows [y0, y1) of the image into a device buffer of
+    (y1 - y0) * width * 3 doubles on a CUDA stream (no sync)."""
+    rec = opts.record()
+    cfg = gpu.record() if gpu is not None else None
+    N.check(N.lib().zt_render_rows_device(scene.handle, N.ptr(rec), int(y0), int(y1),
+                                          N.ptr(cfg) if cfg is not None else None, C.c_void_p(d_out_ptr),
+                                          C.c_void_p(stream_ptr)))
+
+
 class Batch:
     """A prepared batch of renders (zt_batch): one persistent launch over all
     images, captured in a CUDA graph and replayed by ``launch``.  Outputs are

@@ -880,15 +880,20 @@ static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t c
   return ZT_OK;
 }
 
-static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* d_out,
-                               cudaStream_t stream) {
-  const RenderParams p = make_params(s, o);
+/* Renders the rows [p.row0, p.row0 + p.rows) of the image into d_out (the
+ * band's rows only).  The wavefront mode renders whole images. */
+static zt_status launch_render_params(zt_scene* s, const RenderParams& p, const zt_gpu_config* cfg, double* d_out,
+                                      cudaStream_t stream) {
   if (p.max_depth == 0) { /* traceWith never enters its loop: every sample is zero */
-    ZT_CUDA(cudaMemsetAsync(d_out, 0, p.width * p.height * 3 * sizeof(double), stream), "clear framebuffer");
+    ZT_CUDA(cudaMemsetAsync(d_out, 0, p.width * p.rows * 3 * sizeof(double), stream), "clear framebuffer");
     return ZT_OK;
   }
   const uint32_t mode = cfg ? cfg->mode : ZT_MODE_AUTO;
-  if (mode == ZT_MODE_WAVEFRONT) return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
+  if (mode == ZT_MODE_WAVEFRONT) {
+    if (p.row0 != 0 || p.rows != p.height)
+      return fail(ZT_ERR_INVALID_ARGUMENT, "the wavefront mode renders whole images, not row bands");
+    return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
+  }
   if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
@@ -898,6 +903,11 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
   const MegaVariant variant =
       (mode == ZT_MODE_MEGAKERNEL_REGEN || (mode == ZT_MODE_AUTO && long_paths)) ? kMegaRegen : kMegaNested;
   return launch_mega(s, p, bs, d_out, variant, use_fast(s, p, precision), stream);
+}
+
+static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* d_out,
+                               cudaStream_t stream) {
+  return launch_render_params(s, make_params(s, o), cfg, d_out, stream);
 }
 
 /* Error word of the last wavefront launch (after the stream is idle). */
@@ -951,6 +961,23 @@ zt_status zt_render_device(zt_scene* s, const zt_options* o, const zt_gpu_config
   if (!s->device || s->device->device != dev)
     return fail(ZT_ERR_INVALID_ARGUMENT, "scene is not resident on the current device: call zt_scene_upload");
   return launch_render(s, o, cfg, d_out, (cudaStream_t)stream);
+}
+
+zt_status zt_render_rows_device(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end,
+                                const zt_gpu_config* cfg, double* d_out, void* stream) {
+  zt_status rc = check_render_args(s, o);
+  if (rc != ZT_OK) return rc;
+  if (!d_out) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_rows_device: NULL output");
+  if (row_begin >= row_end || row_end > o->height)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_render_rows_device: need row_begin < row_end <= height");
+  int dev = 0;
+  ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (!s->device || s->device->device != dev)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "scene is not resident on the current device: call zt_scene_upload");
+  RenderParams p = make_params(s, o); /* camera and RNG streams of the whole image */
+  p.row0 = row_begin;
+  p.rows = row_end - row_begin;
+  return launch_render_params(s, p, cfg, d_out, (cudaStream_t)stream);
 }
 
 zt_status zt_render_ex(zt_scene* s, const zt_options* o, const zt_gpu_config* cfg, double* out) {

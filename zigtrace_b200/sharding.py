@@ -1,9 +1,10 @@
 """Work split across GPUs, one process per GPU.
 
 Pixels are independent (each owns its RNG stream, src/render.zig:135), so
-rank r renders a contiguous band of image rows with zt_render_rows and the
-bands are gathered with one all-gather over torch.distributed (NCCL on GPUs,
-gloo on CPU).  The gathered image is bit-identical to a one-device render.
+rank r renders a contiguous band of image rows straight into its slot of a
+device buffer (zt_render_rows_device) and one all-gather over
+torch.distributed (NCCL on GPUs, gloo on CPU) assembles the frame in device
+memory.  The gathered image is bit-identical to a one-device render.
 Bands can be balanced by a per-row cost estimate (e.g. the previous frame's
 per-row times); without one they split the rows evenly.
 
@@ -11,7 +12,8 @@ The differentiable form splits the same way: each rank runs the forward and
 the path-replay backward of its band (zt_forward_rows / zt_backward_rows)
 and one all-reduce sums the gradient shares (3 values per material).  A
 batch of renders is split by estimated cost, longest first onto the least
-loaded rank (LPT), and the images are gathered on every rank.
+loaded rank (LPT), rendered as one batched launch per rank, and gathered
+with one tensor all-gather on every rank.
 """
 from __future__ import annotations
 
@@ -46,39 +48,71 @@ def row_bands(height: int, world: int, row_costs: Optional[Sequence[float]] = No
 
 
 def render_rows(scene: Scene, opts: Options, y0: int, y1: int) -> np.ndarray:
-    """Rows [y0, y1) of the image on the current device ((y1-y0)*width x 3)."""
+    """Rows [y0, y1) of the image on the current device, into host memory
+    ((y1-y0)*width x 3)."""
     out = np.zeros(max(y1 - y0, 0) * int(opts.width) * 3 + 1, np.float64)  # the C ABI validates the band
     N.check(N.lib().zt_render_rows(scene.handle, N.ptr(opts.record()), y0, y1, N.ptr(out)))
     return out[:-1].reshape(-1, 3)
 
 
+def _device(group):
+    import torch
+    import torch.distributed as dist
+    return torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+
+
+def _gather_padded(buf, world: int, group):
+    """All-gather of equal-sized flat tensors into one (world * len) tensor:
+    all_gather_into_tensor on NCCL, the list form elsewhere (gloo)."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        out = torch.empty(world * buf.numel(), dtype=buf.dtype, device=buf.device)
+        dist.all_gather_into_tensor(out, buf, group=group)
+        return out
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return torch.cat(parts)
+
+
 def render_sharded(scene: Scene, opts: Options, group=None,
-                   render_band: Callable[[Scene, Options, int, int], np.ndarray] = render_rows,
-                   row_costs: Optional[Sequence[float]] = None) -> np.ndarray:
-    """Renders the image across the ranks of `group` and returns the whole
-    (height*width x 3) image on every rank."""
+                   render_band: Optional[Callable[[Scene, Options, int, int], np.ndarray]] = None,
+                   row_costs: Optional[Sequence[float]] = None, gpu=None, as_numpy: bool = True, stream=None):
+    """Renders the image across the ranks of `group`; every rank gets the
+    whole (height*width x 3) image.
+
+    By default each rank renders its band on its GPU straight into its slot
+    of the all-gather buffer (zt_render_rows_device) and one all-gather
+    assembles the frame in device memory, with no host round trip; with
+    as_numpy=False the image stays on the device (a torch tensor).
+    `render_band` substitutes another band renderer returning host rows
+    (the CPU tests use the oracle)."""
     import torch
     import torch.distributed as dist
 
+    from .api import render_rows_device
+
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    bands = row_bands(int(opts.height), world, row_costs)
+    height, width = int(opts.height), int(opts.width)
+    bands = row_bands(height, world, row_costs)
     y0, y1 = bands[rank]
-    width = int(opts.width)
-    mine = render_band(scene, opts, y0, y1) if y1 > y0 else np.zeros((0, 3))
     max_rows = max(b - a for a, b in bands)
-    device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
-        else torch.device("cpu")
+    device = _device(group)
     buf = torch.zeros(max_rows * width * 3, dtype=torch.float64, device=device)
-    if len(mine):
-        buf[:mine.size] = torch.from_numpy(np.ascontiguousarray(mine).reshape(-1)).to(device)
-    parts = [torch.empty_like(buf) for _ in range(world)]
-    dist.all_gather(parts, buf, group=group)
-    img = np.empty((int(opts.height) * width, 3), np.float64)
-    for (a, b), part in zip(bands, parts):
-        n = (b - a) * width
-        img[a * width:b * width] = part[:n * 3].cpu().numpy().reshape(-1, 3)
-    return img
+    if y1 > y0:
+        if render_band is not None:
+            mine = np.ascontiguousarray(render_band(scene, opts, y0, y1), np.float64).reshape(-1)
+            buf[:mine.size] = torch.from_numpy(mine).to(device)
+        else:
+            st = stream if stream is not None else torch.cuda.current_stream()
+            render_rows_device(scene, opts, y0, y1, buf.data_ptr(), st.cuda_stream, gpu)
+    gathered = _gather_padded(buf, world, group)
+    stride = max_rows * width * 3
+    img = torch.cat([gathered[r * stride:r * stride + (b - a) * width * 3] for r, (a, b) in enumerate(bands)])
+    img = img.view(height * width, 3)
+    return img.cpu().numpy() if as_numpy else img
 
 
 def forward_sharded(scene: Scene, opts: Options, colors=None, group=None, row_costs=None,
@@ -139,21 +173,54 @@ def batch_costs(scenes: Sequence[Scene], opts_list: Sequence[Options]) -> List[f
 
 def render_batch_sharded(scenes: Sequence[Scene], opts_list: Sequence[Options], group=None,
                          costs: Optional[Sequence[float]] = None,
-                         render_item: Optional[Callable] = None) -> List[np.ndarray]:
+                         render_item: Optional[Callable] = None, gpu=None, as_numpy: bool = True):
     """Renders a batch across the ranks of `group` (LPT by cost) and returns
-    every image (height*width x 3), in input order, on every rank."""
+    every image (height*width x 3), in input order, on every rank.
+
+    Each rank renders its renders as one persistent batched launch into one
+    flat device buffer (its images back to back, in index order); the
+    buffers, padded to the largest, are gathered with one tensor all-gather,
+    and every rank cuts the images out of the result (all ranks know the
+    assignment and the sizes).  `render_item` substitutes another renderer
+    returning host arrays (the CPU tests)."""
+    import torch
     import torch.distributed as dist
+
+    from .api import Batch
 
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     costs = batch_costs(scenes, opts_list) if costs is None else costs
-    mine = assign_batch(costs, world)[rank]
-    fn = render_item or (lambda sc, o: render(sc, o).pixels)
-    local = {i: np.ascontiguousarray(fn(scenes[i], opts_list[i])) for i in mine}
-    gathered: list = [None] * world
-    dist.all_gather_object(gathered, local, group=group)
-    images: List[Optional[np.ndarray]] = [None] * len(scenes)
-    for part in gathered:
-        for i, img in part.items():
-            images[i] = img
-    return images  # type: ignore[return-value]
+    parts = assign_batch(costs, world)
+    sizes = [int(o.width) * int(o.height) * 3 if not isinstance(o, tuple) else int(o[0]) * int(o[1]) * 3
+             for o in opts_list]
+    totals = [sum(sizes[i] for i in p) for p in parts]
+    device = _device(group)
+    buf = torch.zeros(max(max(totals), 1), dtype=torch.float64, device=device)
+    mine = parts[rank]
+    offs, cur = {}, 0
+    for i in mine:
+        offs[i] = cur
+        cur += sizes[i]
+    if mine:
+        if render_item is not None:
+            for i in mine:
+                img = np.ascontiguousarray(render_item(scenes[i], opts_list[i]), np.float64).reshape(-1)
+                buf[offs[i]:offs[i] + sizes[i]] = torch.from_numpy(img).to(device)
+        else:
+            for i in mine:
+                scenes[i].upload()
+            batch = Batch([scenes[i] for i in mine], [opts_list[i] for i in mine],
+                          [buf.data_ptr() + 8 * offs[i] for i in mine], gpu)
+            batch.launch(torch.cuda.current_stream().cuda_stream)
+            batch.close()
+    gathered = _gather_padded(buf, world, group)
+    stride = buf.numel()
+    images: list = [None] * len(scenes)
+    for r, p in enumerate(parts):
+        cur = r * stride
+        for i in p:
+            img = gathered[cur:cur + sizes[i]].view(-1, 3)
+            images[i] = img.cpu().numpy() if as_numpy else img
+            cur += sizes[i]
+    return images

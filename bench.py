@@ -86,6 +86,8 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size in seconds")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="use --mode as given instead of the autotuner's choice")
     p.add_argument("--no-extras", action="store_true",
                    help="default workload only: skip the batch and diff sub-objects")
     p.add_argument("--mode", type=int, default=0, help="zt_gpu_config.mode")
@@ -313,6 +315,14 @@ def b200_arm(args):
     scene.upload()
     prec = zt.PRECISION_FAST if args.precision == "fast" else zt.PRECISION_EXACT
     gcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity, precision=prec)
+    tuned = None
+    if args.autotune:  # mode, block size and queue capacity from the project's autotuner
+        from zigtrace_b200 import autotune
+        gcfg, tune_ms, tune_cached = autotune.tune_render(scene, o, reps=1, precision=prec)
+        tuned = {"mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][gcfg.mode],
+                 "block_size": gcfg.block_size, "queue_capacity": gcfg.queue_capacity, "precision": args.precision,
+                 "cached": tune_cached, "candidates_ms": tune_ms,
+                 "candidate_key": "[mode, block_size, queue_capacity]"}
     npix = o.width * o.height
     samples = npix * o.spp
     out = torch.empty(npix * 3, dtype=torch.float64, device="cuda")
@@ -357,7 +367,8 @@ def b200_arm(args):
     if prec == zt.PRECISION_FAST and not args.no_extras:
         # the verification build (bit-identical to the reference algorithm) on
         # the same frame, timed the same way
-        vcfg = zt.GpuConfig(mode=args.mode, queue_capacity=args.capacity, precision=zt.PRECISION_EXACT)
+        vcfg = zt.GpuConfig(mode=gcfg.mode, block_size=gcfg.block_size, queue_capacity=gcfg.queue_capacity,
+                            precision=zt.PRECISION_EXACT)
         for _ in range(args.warmup):
             flush.zero_()
             zt.render_device(scene, o, out.data_ptr(), stream.cuda_stream, vcfg)
@@ -424,10 +435,10 @@ def b200_arm(args):
         roofline = roofline_entry(
             work, samples, kernel_ms, sms,
             (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
-             if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and args.mode in (0, 1) else None),
+             if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and gcfg.mode in (0, 1) else None),
             "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
-            NCU_EXECUTION.get(args.workload) if args.mode in (0, 1) else None)
-        if args.mode == 2:  # the wavefront form: path-state traffic through HBM against the copy peak
+            NCU_EXECUTION.get(args.workload) if gcfg.mode in (0, 1) else None)
+        if gcfg.mode == 2:  # the wavefront form: path-state traffic through HBM against the copy peak
             qbps = queue_bytes * samples / (kernel_ms / 1e3) / 1e9
             roofline["queue"] = {"bytes_per_sample": round(queue_bytes, 1), "achieved_gbs": round(qbps, 1),
                                  "peak_gbs": roofline["memory"]["peak_gbs"],
@@ -440,8 +451,8 @@ def b200_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
-                   "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][args.mode],
-                   "precision": args.precision,
+                   "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][gcfg.mode],
+                   "precision": args.precision, "autotune": tuned,
                    "sharding": "one frame per rank (seed = rank), no collective",
                    "bvh_build": {"on_device": scene.built_on_device,
                                  "device_ms": round(scene.build_ms, 2) if scene.build_ms else None}},
@@ -558,14 +569,20 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
         s.upload()
     samples = sum(o.width * o.height * o.spp for o in opts)
     outs = [torch.empty(o.width * o.height * 3, dtype=torch.float64, device="cuda") for o in opts]
-    cfg, order, tune_ms, cached = autotune.tune_batch(scs, opts, reps=1)
+    prec = zt.PRECISION_FAST if args.precision == "fast" else zt.PRECISION_EXACT
+    cfg, order, tune_ms, cached = autotune.tune_batch(scs, opts, reps=1, precision=prec)
+    plain_won = order == autotune.PLAIN
+    if plain_won:  # still measure the best batched launch against the plain launches
+        best = min((k for k in tune_ms if json.loads(k)[0] != autotune.PLAIN), key=tune_ms.get)
+        cfg, order = zt.GpuConfig(block_size=json.loads(best)[0], precision=prec), json.loads(best)[1]
     batch = zt.Batch(scs, opts, [t.data_ptr() for t in outs], cfg, order)
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def plain():
         for s, o, t in zip(scs, opts, outs):
-            zt.render_device(s, o, t.data_ptr(), stream.cuda_stream, zt.GpuConfig(block_size=cfg.block_size))
+            zt.render_device(s, o, t.data_ptr(), stream.cuda_stream,
+                             zt.GpuConfig(block_size=cfg.block_size, precision=prec))
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -617,7 +634,7 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
                "d2h_bytes_per_step": sum(o.width * o.height * 24 for o in opts)}
         same_e2e = all(torch.equal(x, t) for x, t in zip(batched_imgs, pinned))
         times = []  # the same 256 renders as one zt_render_ex call each, into the same pinned buffers
-        pcfg = zt.GpuConfig(block_size=cfg.block_size).record()
+        pcfg = zt.GpuConfig(block_size=cfg.block_size, precision=prec).record()
         orecs = [o.record() for o in opts]
         for i in range(args.warmup + args.steps):
             for s in scs:
@@ -676,8 +693,10 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
                                "resolution from {64x64, 128x128, 256x256, 512x288}, 16 spp, depth 16, NEE on",
                    "renders": len(items), "samples_per_step": samples,
                    "l2": "flushed by a 256 MB write before every step",
+                   "precision": args.precision,
                    "autotune": {"block_size": cfg.block_size, "order": ["given", "largest_first"][order],
-                                "cached": cached, "candidates_ms": tune_ms},
+                                "plain_launches_won": plain_won, "cached": cached, "candidates_ms": tune_ms,
+                                "candidate_key": "[block_size, order]; [-1, 0] = plain per-render launches"},
                    "sharding": "one batch per rank (seeds offset by rank), no collective"},
         "plain_launches": {"value": round(plain_value, 4), "unit": "Msamples/s", "ms_per_step": round(plain_ms, 3),
                            "launches_per_step": len(items)},

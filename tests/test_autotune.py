@@ -24,10 +24,24 @@ def test_choose_picks_fastest_and_caches(tmp_path, monkeypatch):
     assert best3 == (1, 128, 0) and not cached3
 
 
+def test_candidates_cover_modes_blocks_and_queue_capacities():
+    modes = {m for m, _, _ in autotune.SINGLE_CANDIDATES}
+    assert modes == {zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN, zt.MODE_WAVEFRONT}
+    caps = {c for m, _, c in autotune.SINGLE_CANDIDATES if m == zt.MODE_WAVEFRONT}
+    assert len(caps) >= 3 and 0 in caps
+    assert {b for m, b, _ in autotune.SINGLE_CANDIDATES if m == zt.MODE_MEGAKERNEL} == {64, 128, 256}
+    assert (autotune.PLAIN, 0) in autotune.BATCH_CANDIDATES
+    assert {o for b, o in autotune.BATCH_CANDIDATES if b != autotune.PLAIN} == {0, 1}
+
+
 def test_scene_class_keys(native_lib):
     s = scenes.cornell().build()
     k = autotune.scene_class(s, zt.Options(256, 256, 64, 16))
-    assert k == "prims1e1|lights1|px1e5|spp64|depth16|nee1"
+    assert k == "prims1e1|planes0|lights1|px1e5|spp64|depth16|nee1|prec0"
+    assert autotune.scene_class(s, zt.Options(256, 256, 64, 16), precision=1).endswith("|prec1")
+    c2 = autotune.scene_class(scenes.random_spheres().build(), scenes.SPHERES_OPTIONS)
+    c3 = autotune.scene_class(scenes.triangle_heavy(nx=100, nz=50).build(), scenes.TRIANGLE_HEAVY_OPTIONS)
+    assert len({k, c2, c3}) == 3 and "planes1" in c2 and "lights0" in c2
     wl = scenes.batch_workload(count=4)
     for sc, _ in wl:
         sc.build()

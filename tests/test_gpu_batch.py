@@ -61,12 +61,15 @@ def test_autotuned_configs_render_identical_pixels(tmp_path, monkeypatch):
     for mode, bs, cap in autotune.SINGLE_CANDIDATES:
         got = zt.render(scene, o, zt.GpuConfig(mode=mode, block_size=bs, queue_capacity=cap)).pixels
         assert got.tobytes() == want.tobytes()
-    cfg = autotune.tune_render(scene, o, reps=1)
+    cfg, ms, cached = autotune.tune_render(scene, o, reps=1)
     assert (cfg.mode, cfg.block_size, cfg.queue_capacity) in autotune.SINGLE_CANDIDATES
+    assert not cached and len(ms) == len(autotune.SINGLE_CANDIDATES)
     assert zt.render(scene, o, cfg).pixels.tobytes() == want.tobytes()
+    fcfg, _, _ = autotune.tune_render(scene, o, reps=1, precision=zt.PRECISION_FAST)  # its own cache entry
+    assert fcfg.precision == zt.PRECISION_FAST
     items = mixed_batch()
     bcfg, order, ms, cached = autotune.tune_batch([s for s, _ in items], [o for _, o in items], reps=1)
-    assert not cached and len(ms) == len(autotune.BATCH_CANDIDATES) and order in (0, 1)
+    assert not cached and len(ms) == len(autotune.BATCH_CANDIDATES) and order in (0, 1, autotune.PLAIN)
     assert autotune.tune_batch([s for s, _ in items], [o for _, o in items], reps=1)[3]  # cached now
 
 

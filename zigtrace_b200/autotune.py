@@ -1,11 +1,18 @@
 """Autotuner for the device execution choices.
 
 For a render it times the megakernel at block sizes 64/128/256, the
-megakernel with path regeneration and the wavefront form; for a batch it times block sizes 64/128/256 with the renders
-in the given order or largest first.  Every candidate renders identical
-pixels (the choice only changes scheduling), so the fastest one is kept.
-Results are cached per (GPU, scene class) in a JSON file, by default
-``~/.cache/zigtrace_b200/autotune.json`` (override with ZT_AUTOTUNE_CACHE).
+megakernel with path regeneration at 128/256, and the wavefront form at
+three queue capacities (paths in flight: the default of one slot per pixel
+up to 4M, 1M and 256K).  For a batch it times the batched persistent launch
+at block sizes 64/128/256 with the renders in the given order or largest
+first, and the same renders as plain per-render launches (each with its own
+default choice) as one more candidate.  Every candidate renders identical
+pixels at the caller's precision (the choice only changes scheduling), so
+the fastest one is kept; the precision itself is the caller's choice and is
+part of the cache key, since the exact and fast builds differ in their best
+configuration.  Results are cached per (GPU, scene class) in a JSON file, by
+default ``~/.cache/zigtrace_b200/autotune.json`` (override with
+ZT_AUTOTUNE_CACHE).
 """
 from __future__ import annotations
 
@@ -20,8 +27,10 @@ from .api import MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, Batch, 
 
 SINGLE_CANDIDATES: List[Tuple[int, int, int]] = [  # (mode, block_size, queue_capacity)
     (MODE_MEGAKERNEL, 64, 0), (MODE_MEGAKERNEL, 128, 0), (MODE_MEGAKERNEL, 256, 0),
-    (MODE_MEGAKERNEL_REGEN, 128, 0), (MODE_WAVEFRONT, 128, 0)]
-BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)]
+    (MODE_MEGAKERNEL_REGEN, 128, 0), (MODE_MEGAKERNEL_REGEN, 256, 0),
+    (MODE_WAVEFRONT, 128, 0), (MODE_WAVEFRONT, 128, 1 << 20), (MODE_WAVEFRONT, 128, 1 << 18)]
+PLAIN = -1  # batch candidate: plain per-render launches instead of the batched launch
+BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)] + [(PLAIN, 0)]
 
 
 def cache_path() -> Path:
@@ -55,18 +64,23 @@ def _mag(x: float) -> int:
     return int(round(math.log10(max(x, 1.0))))
 
 
-def scene_class(scene: Scene, opts: Options) -> str:
+def scene_class(scene: Scene, opts: Options, precision: int = 0) -> str:
     """Coarse class of a render: orders of magnitude of primitives and
-    pixels, whether it has lights, spp, depth, light sampling."""
+    pixels, whether it has lights and planes, spp, depth, light sampling and
+    precision.  The Cornell box (1e1 primitives, lights, 256x256x64), the
+    random spheres (1e2, a plane, no lights, depth 50) and the 1M-triangle
+    terrain (1e6, lights) fall in different classes."""
     c = scene.counts()
-    return (f"prims1e{_mag(c['bounded'] + c['planes'])}|lights{int(c['lights'] > 0)}|px1e{_mag(opts.width * opts.height)}"
-            f"|spp{opts.spp}|depth{opts.max_depth}|nee{int(opts.light_sampling)}")
+    return (f"prims1e{_mag(c['bounded'] + c['planes'])}|planes{int(c['planes'] > 0)}|lights{int(c['lights'] > 0)}"
+            f"|px1e{_mag(opts.width * opts.height)}|spp{opts.spp}|depth{opts.max_depth}"
+            f"|nee{int(opts.light_sampling)}|prec{precision}")
 
 
-def batch_class(scenes: Sequence[Scene], opts: Sequence[Options]) -> str:
+def batch_class(scenes: Sequence[Scene], opts: Sequence[Options], precision: int = 0) -> str:
     px = sum(o.width * o.height for o in opts)
     prims = sum(s.counts()["bounded"] for s in scenes) / len(scenes)
-    return f"batch|n{len(scenes)}|px1e{_mag(px)}|meanprims1e{_mag(prims)}|spp{opts[0].spp}|depth{opts[0].max_depth}"
+    return (f"batch|n{len(scenes)}|px1e{_mag(px)}|meanprims1e{_mag(prims)}|spp{opts[0].spp}"
+            f"|depth{opts[0].max_depth}|prec{precision}")
 
 
 def _event_timer(fn: Callable[[], None], reps: int) -> float:
@@ -102,36 +116,51 @@ def choose(key: str, candidates: Sequence, run: Callable, reps: int = 2, use_cac
     return tuple(json.loads(best)), ms, False
 
 
-def tune_render(scene: Scene, opts: Options, reps: int = 2, use_cache: bool = True) -> GpuConfig:
-    """Fastest device configuration for rendering `scene` with `opts`."""
+def tune_render(scene: Scene, opts: Options, reps: int = 2, use_cache: bool = True, precision: int = 0,
+                candidates: Optional[Sequence[Tuple[int, int, int]]] = None) -> Tuple[GpuConfig, Dict, bool]:
+    """Fastest device configuration for rendering `scene` with `opts` at
+    `precision`; returns (config, timings in ms per candidate, whether the
+    choice came from the cache)."""
     import torch
     scene.upload()
     out = torch.empty(opts.width * opts.height * 3, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
 
     def run(c):
-        render_device(scene, opts, out.data_ptr(), stream, GpuConfig(mode=c[0], block_size=c[1], queue_capacity=c[2]))
+        render_device(scene, opts, out.data_ptr(), stream,
+                      GpuConfig(mode=c[0], block_size=c[1], queue_capacity=c[2], precision=precision))
 
-    best, _, _ = choose(f"{gpu_key()}|render|{scene_class(scene, opts)}", SINGLE_CANDIDATES, run, reps, use_cache)
-    return GpuConfig(mode=best[0], block_size=best[1], queue_capacity=best[2])
+    best, ms, cached = choose(f"{gpu_key()}|render|{scene_class(scene, opts, precision)}",
+                              candidates or SINGLE_CANDIDATES, run, reps, use_cache)
+    del out
+    return GpuConfig(mode=best[0], block_size=best[1], queue_capacity=best[2], precision=precision), ms, cached
 
 
 def tune_batch(scenes: Sequence[Scene], opts: Sequence[Options], reps: int = 2,
-               use_cache: bool = True) -> Tuple[GpuConfig, int, Dict, bool]:
-    """Fastest (block size, order) for a batch; returns (config, order,
-    timings in ms, whether it came from the cache)."""
+               use_cache: bool = True, precision: int = 0) -> Tuple[GpuConfig, int, Dict, bool]:
+    """Fastest (block size, order) for a batch at `precision`; order is PLAIN
+    when per-render launches beat every batched launch.  Returns (config,
+    order, timings in ms, whether it came from the cache)."""
     import torch
     outs = [torch.empty(o.width * o.height * 3, dtype=torch.float64, device="cuda") for o in opts]
     stream = torch.cuda.current_stream().cuda_stream
     batches = {}
 
     def run(c):
+        if c[0] == PLAIN:
+            for s, o, t in zip(scenes, opts, outs):
+                render_device(s, o, t.data_ptr(), stream, GpuConfig(precision=precision))
+            return
         if c not in batches:
-            batches[c] = Batch(scenes, opts, [t.data_ptr() for t in outs], GpuConfig(block_size=c[0]), order=c[1])
+            batches[c] = Batch(scenes, opts, [t.data_ptr() for t in outs],
+                               GpuConfig(block_size=c[0], precision=precision), order=c[1])
         batches[c].launch(stream)
 
-    best, ms, cached = choose(f"{gpu_key()}|{batch_class(scenes, opts)}", BATCH_CANDIDATES, run, reps, use_cache)
+    best, ms, cached = choose(f"{gpu_key()}|{batch_class(scenes, opts, precision)}", BATCH_CANDIDATES, run, reps,
+                              use_cache)
     torch.cuda.synchronize()
     for b in batches.values():
         b.close()
-    return GpuConfig(block_size=best[0]), best[1], ms, cached
+    if best[0] == PLAIN:
+        return GpuConfig(precision=precision), PLAIN, ms, cached
+    return GpuConfig(block_size=best[0], precision=precision), best[1], ms, cached

@@ -187,6 +187,13 @@ zt_status zt_render_ex(zt_scene* scene, const zt_options* opts, const zt_gpu_con
  * must have been uploaded to the current device. */
 zt_status zt_render_device(zt_scene* scene, const zt_options* opts, const zt_gpu_config* cfg,
                            double* d_out_rgb, void* stream);
+/* Upper bound on the iterations of the wavefront loop, which runs on the
+ * device (a CUDA-graph while node): a render that reaches it stops and its
+ * zt_render / zt_render_ex call returns ZT_ERR_TIMEOUT.  The default (0)
+ * bound is pixels x spp x (max_depth + 1), which no correct render reaches;
+ * a lower one makes the bound fire, to exercise that error path.
+ * Process-wide. */
+zt_status zt_set_wavefront_iteration_limit(uint64_t max_iterations);
 /* Device-resident band: rows [row_begin, row_end) of the width x height
  * image (the same camera and per-pixel RNG streams, so the band equals those
  * rows of the whole image) into the device buffer d_out_rgb of

@@ -238,3 +238,23 @@ def test_fuzz_scenes_without_light_sampling_bit_exact(seed, mode):
     img = zt.render(scene, o, zt.GpuConfig(mode)).pixels
     want = O.OracleScene.from_scene(scene).render(32, 20, 3, 12, seed=seed, light_sampling=False)
     assert img.tobytes() == want.tobytes()
+
+
+def test_wavefront_iteration_bound_returns_timeout():
+    """The wavefront loop runs on the device under an iteration bound; lowered
+    below what the render needs, the bound ends the loop and the call returns
+    ZT_ERR_TIMEOUT instead of hanging; the next render at the default bound
+    is bit-exact again."""
+    from zigtrace_b200 import _native as N
+    scene = scenes.cornell().build()
+    o = zt.Options(64, 64, 4, 16)
+    g = zt.GpuConfig(zt.MODE_WAVEFRONT)
+    N.check(N.lib().zt_set_wavefront_iteration_limit(3))
+    try:
+        with pytest.raises(zt.ZigtraceError) as ei:
+            zt.render(scene, o, g)
+        assert ei.value.name == "Timeout" and "iteration bound" in str(ei.value)
+    finally:
+        N.check(N.lib().zt_set_wavefront_iteration_limit(0))
+    want = O.OracleScene.from_scene(scene).render(64, 64, 4, 16)
+    assert zt.render(scene, o, g).pixels.tobytes() == want.tobytes()

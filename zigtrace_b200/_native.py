@@ -77,6 +77,7 @@ SIGNATURES = {
     "zt_render_rows": (_i32, [_P, _P, _u64, _u64, _P]),
     "zt_render_device": (_i32, [_P, _P, _P, _P, _P]),
     "zt_render_rows_device": (_i32, [_P, _P, _u64, _u64, _P, _P, _P]),
+    "zt_set_wavefront_iteration_limit": (_i32, [_u64]),
     "zt_render_debug": (_i32, [_P, _P, _P, _P]),
     "zt_render_noalloc": (_i32, [_P, _P, _P, _P]),
     "zt_forward": (_i32, [_P, _P, _P, _P]),

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <string>
@@ -48,7 +49,7 @@ struct zt_wavefront_cache {
   zt::WfState state;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t done = nullptr;  /* recorded after the last launch of exec */
-  unsigned char key[sizeof(zt::DevScene) + sizeof(zt::RenderParams) + 2 * sizeof(void*)] = {};
+  unsigned char key[sizeof(zt::DevScene) + sizeof(zt::RenderParams) + sizeof(void*) + 2 * sizeof(uint64_t)] = {};
 };
 
 /* The per-sample primal radiance of the last zt_forward, with everything it
@@ -327,6 +328,7 @@ constexpr int kMegaThreadsPerSmNoNee = 896;
 template <int BS, bool kNee, bool kFast = false>
 __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
     k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out, unsigned int* __restrict__ counter) {
+  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
@@ -435,6 +437,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
 template <int BS, bool kFast = false>
 __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
                                                              unsigned int* __restrict__ counter) {
+  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
@@ -468,6 +471,7 @@ template <int BS, bool kNee, bool kFast = false>
 __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
     k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
                    unsigned int* __restrict__ counter) {
+  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const unsigned lane = threadIdx.x & 31;
   for (;;) {
     unsigned tile = 0;
@@ -701,9 +705,9 @@ static int sm_count() {
 }
 
 template <typename K>
-static unsigned persistent_grid(K kernel, int block, uint64_t work_items) {
+static unsigned persistent_grid(K kernel, int block, uint64_t work_items, size_t smem = 0) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   uint64_t blocks = (uint64_t)sm_count() * per_sm;
   const uint64_t need = (work_items + block - 1) / block;
@@ -721,15 +725,16 @@ template <int BS, bool kFast>
 static void launch_mega_bsf(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
                             MegaVariant variant, cudaStream_t stream) {
   const uint64_t npix = p.width * p.rows;
+  const size_t smem = kFast ? fast_stack_bytes(BS) : 0; /* the fast walk's shared stack */
   if (variant == kMegaRegen)
-    k_render_regen<BS, kFast><<<persistent_grid(k_render_regen<BS, kFast>, BS, npix), BS, 0, stream>>>(v, p, d_out,
-                                                                                                      counter);
+    k_render_regen<BS, kFast><<<persistent_grid(k_render_regen<BS, kFast>, BS, npix, smem), BS, smem, stream>>>(
+        v, p, d_out, counter);
   else if (p.use_nee)
-    k_render_mega<BS, true, kFast><<<persistent_grid(k_render_mega<BS, true, kFast>, BS, npix), BS, 0, stream>>>(
-        v, p, d_out, counter);
+    k_render_mega<BS, true, kFast><<<persistent_grid(k_render_mega<BS, true, kFast>, BS, npix, smem), BS, smem,
+                                     stream>>>(v, p, d_out, counter);
   else
-    k_render_mega<BS, false, kFast><<<persistent_grid(k_render_mega<BS, false, kFast>, BS, npix), BS, 0, stream>>>(
-        v, p, d_out, counter);
+    k_render_mega<BS, false, kFast><<<persistent_grid(k_render_mega<BS, false, kFast>, BS, npix, smem), BS, smem,
+                                      stream>>>(v, p, d_out, counter);
 }
 
 template <int BS>
@@ -809,7 +814,7 @@ static zt_status wavefront_state(zt_device_buffers* d, uint32_t cap) {
 /* Builds the executable graph: while (queue not empty) { extend; shade;
  * shadow; advance }.  The loop runs on the device; the host never waits. */
 static zt_status build_wavefront_graph(const DevScene& view, const RenderParams& p, const WfState& w, double* d_out,
-                                       cudaGraphExec_t* exec_out) {
+                                       uint64_t max_iter, cudaGraphExec_t* exec_out) {
   cudaGraph_t g = nullptr;
   cudaStream_t cs = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -831,9 +836,6 @@ static zt_status build_wavefront_graph(const DevScene& view, const RenderParams&
       k_wf_extend<<<persistent_grid(k_wf_extend, 128, cap), 128, 0, cs>>>(view, w);
       k_wf_shade<<<persistent_grid(k_wf_shade, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
       k_wf_shadow<<<persistent_grid(k_wf_shadow, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
-      /* every iteration advances each active slot by one bounce: a bound */
-      const double bound = (double)(p.width * p.height) * (double)p.spp * (double)(p.max_depth + 1) + 16.0;
-      const uint64_t max_iter = bound > 4.0e9 ? 4000000000ull : (uint64_t)bound;
       k_wf_advance<<<1, 1, 0, cs>>>(w, h, max_iter);
       cudaGraph_t captured = nullptr;
       cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
@@ -846,6 +848,20 @@ static zt_status build_wavefront_graph(const DevScene& view, const RenderParams&
   if (e != cudaSuccess) return cuda_fail(e, "build wavefront graph");
   *exec_out = exec;
   return ZT_OK;
+}
+
+/* Iteration bound of the wavefront loop: every iteration advances each
+ * active slot by one bounce, so pixels x spp x (max_depth + 1) iterations
+ * finish any render; g_wf_iteration_limit (zt_set_wavefront_iteration_limit)
+ * can lower it to exercise the bound's error path. */
+static std::atomic<uint64_t> g_wf_iteration_limit{0};
+
+static uint64_t wavefront_max_iter(const RenderParams& p) {
+  const double bound = (double)(p.width * p.height) * (double)p.spp * (double)(p.max_depth + 1) + 16.0;
+  uint64_t max_iter = bound > 4.0e9 ? 4000000000ull : (uint64_t)bound;
+  const uint64_t lim = g_wf_iteration_limit.load();
+  if (lim && lim < max_iter) max_iter = lim;
+  return max_iter;
 }
 
 static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t capacity, double* d_out,
@@ -862,12 +878,13 @@ static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t c
   memcpy(key, &view, sizeof view);
   memcpy(key + sizeof view, &p, sizeof p);
   memcpy(key + sizeof view + sizeof p, &d_out, sizeof d_out);
-  const uint64_t capk = cap;
-  memcpy(key + sizeof view + sizeof p + sizeof d_out, &capk, sizeof(void*));
+  const uint64_t capk = cap, max_iter = wavefront_max_iter(p);
+  memcpy(key + sizeof view + sizeof p + sizeof d_out, &capk, sizeof capk);
+  memcpy(key + sizeof view + sizeof p + sizeof d_out + sizeof capk, &max_iter, sizeof max_iter);
   if (!c.exec || memcmp(key, c.key, sizeof key) != 0) {
     if (c.done) cudaEventSynchronize(c.done);
     if (c.exec) { cudaGraphExecDestroy(c.exec); c.exec = nullptr; }
-    rc = build_wavefront_graph(view, p, c.state, d_out, &c.exec);
+    rc = build_wavefront_graph(view, p, c.state, d_out, max_iter, &c.exec);
     if (rc != ZT_OK) return rc;
     memcpy(c.key, key, sizeof key);
     if (!c.done) ZT_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "create event");
@@ -961,6 +978,11 @@ zt_status zt_render_device(zt_scene* s, const zt_options* o, const zt_gpu_config
   if (!s->device || s->device->device != dev)
     return fail(ZT_ERR_INVALID_ARGUMENT, "scene is not resident on the current device: call zt_scene_upload");
   return launch_render(s, o, cfg, d_out, (cudaStream_t)stream);
+}
+
+zt_status zt_set_wavefront_iteration_limit(uint64_t max_iterations) {
+  g_wf_iteration_limit.store(max_iterations);
+  return ZT_OK;
 }
 
 zt_status zt_render_rows_device(zt_scene* s, const zt_options* o, uint64_t row_begin, uint64_t row_end,
@@ -1501,8 +1523,9 @@ namespace zt {
 
 template <int BS, bool kNee, bool kFast>
 static void launch_batch_kernel(const zt_batch* b, cudaStream_t st) {
+  const size_t smem = kFast ? fast_stack_bytes(BS) : 0; /* the fast walk's shared stack */
   k_render_batch<BS, kNee, kFast>
-      <<<persistent_grid(k_render_batch<BS, kNee, kFast>, BS, b->total_tiles * 32), BS, 0, st>>>(
+      <<<persistent_grid(k_render_batch<BS, kNee, kFast>, BS, b->total_tiles * 32, smem), BS, smem, st>>>(
           b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
 }
 

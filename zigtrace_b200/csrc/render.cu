@@ -324,11 +324,18 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
  * with its own residency. */
 constexpr int kMegaThreadsPerSm = 896;
 constexpr int kMegaThreadsPerSmNoNee = 896;
+#ifndef ZT_FAST_THREADS_PER_SM
+#define ZT_FAST_THREADS_PER_SM 896
+#endif
+/* Resident threads per SM each megakernel and batch instance is built for
+ * (__launch_bounds__): sets the register budget, 65,536 / threads. */
+__host__ __device__ constexpr int mega_threads_per_sm(bool nee, bool fast) {
+  return fast ? ZT_FAST_THREADS_PER_SM : (nee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee);
+}
 
 template <int BS, bool kNee, bool kFast = false>
-__global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
+__global__ void __launch_bounds__(BS, mega_threads_per_sm(kNee, kFast) / BS)
     k_render_mega(DevScene sc, RenderParams p, double* __restrict__ out, unsigned int* __restrict__ counter) {
-  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
@@ -437,7 +444,6 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
 template <int BS, bool kFast = false>
 __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, RenderParams p, double* __restrict__ out,
                                                              unsigned int* __restrict__ counter) {
-  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const uint64_t tiles_x = (p.width + 7) / 8, tiles = tiles_x * ((p.rows + 3) / 4);
   const uint64_t row_end = p.row0 + p.rows;
   const unsigned lane = threadIdx.x & 31;
@@ -453,13 +459,16 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, Rend
 
 /* One render of a batch: its scene view, parameters, output and the index
  * of its first tile in the batch-wide tile numbering. */
-struct BatchItem {
+struct __align__(16) BatchItem {
   DevScene sc;
   RenderParams p;
   double* out;
   uint64_t tile_begin;
   uint64_t tiles_x;
 };
+#ifndef ZT_BATCH_STAGE_ITEM
+#define ZT_BATCH_STAGE_ITEM 0
+#endif
 
 /* Batched persistent launch: many renders of uneven size share one grid.
  * Warps take 8x4 tiles from one counter over the concatenated tile ranges of
@@ -468,11 +477,14 @@ struct BatchItem {
  * not leave the GPU idle the way one launch per image does.  kNee = false
  * is the instance for batches in which no render samples lights. */
 template <int BS, bool kNee, bool kFast = false>
-__global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee) / BS)
+__global__ void __launch_bounds__(BS, mega_threads_per_sm(kNee, kFast) / BS)
     k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
                    unsigned int* __restrict__ counter) {
-  if (kFast && !fast_stack_ok()) return; /* launched without the fast walk's shared stack: render nothing */
   const unsigned lane = threadIdx.x & 31;
+#if ZT_BATCH_STAGE_ITEM
+  __shared__ __align__(16) BatchItem s_items[BS / 32];
+  uint32_t cur_item = 0xFFFFFFFFu;
+#endif
   for (;;) {
     unsigned tile = 0;
     if (lane == 0) tile = atomicAdd(counter, 1u);
@@ -484,7 +496,22 @@ __global__ void __launch_bounds__(BS, (kNee ? kMegaThreadsPerSm : kMegaThreadsPe
       if (items[mid].tile_begin <= tile) lo = mid;
       else hi = mid - 1;
     }
+#if ZT_BATCH_STAGE_ITEM
+    /* the warp's render, copied into shared memory when it changes: its
+     * scene view and parameters are read on every traversal step, and a
+     * shared copy keeps them out of L1's way */
+    BatchItem& it = s_items[threadIdx.x >> 5];
+    if (lo != cur_item) {
+      __syncwarp();
+      const uint4* src = reinterpret_cast<const uint4*>(items + lo);
+      uint4* dst = reinterpret_cast<uint4*>(&it);
+      for (uint32_t k = lane; k < sizeof(BatchItem) / sizeof(uint4); k += 32) dst[k] = __ldg(src + k);
+      __syncwarp();
+      cur_item = lo;
+    }
+#else
     const BatchItem& it = items[lo];
+#endif
     const uint64_t local = tile - it.tile_begin;
     const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
     if (x < it.p.width && y < it.p.height)
@@ -725,16 +752,15 @@ template <int BS, bool kFast>
 static void launch_mega_bsf(const DevScene& v, const RenderParams& p, double* d_out, unsigned int* counter,
                             MegaVariant variant, cudaStream_t stream) {
   const uint64_t npix = p.width * p.rows;
-  const size_t smem = kFast ? fast_stack_bytes(BS) : 0; /* the fast walk's shared stack */
   if (variant == kMegaRegen)
-    k_render_regen<BS, kFast><<<persistent_grid(k_render_regen<BS, kFast>, BS, npix, smem), BS, smem, stream>>>(
-        v, p, d_out, counter);
+    k_render_regen<BS, kFast><<<persistent_grid(k_render_regen<BS, kFast>, BS, npix), BS, 0, stream>>>(v, p, d_out,
+                                                                                                      counter);
   else if (p.use_nee)
-    k_render_mega<BS, true, kFast><<<persistent_grid(k_render_mega<BS, true, kFast>, BS, npix, smem), BS, smem,
-                                     stream>>>(v, p, d_out, counter);
+    k_render_mega<BS, true, kFast><<<persistent_grid(k_render_mega<BS, true, kFast>, BS, npix), BS, 0, stream>>>(
+        v, p, d_out, counter);
   else
-    k_render_mega<BS, false, kFast><<<persistent_grid(k_render_mega<BS, false, kFast>, BS, npix, smem), BS, smem,
-                                      stream>>>(v, p, d_out, counter);
+    k_render_mega<BS, false, kFast><<<persistent_grid(k_render_mega<BS, false, kFast>, BS, npix), BS, 0, stream>>>(
+        v, p, d_out, counter);
 }
 
 template <int BS>
@@ -1523,9 +1549,8 @@ namespace zt {
 
 template <int BS, bool kNee, bool kFast>
 static void launch_batch_kernel(const zt_batch* b, cudaStream_t st) {
-  const size_t smem = kFast ? fast_stack_bytes(BS) : 0; /* the fast walk's shared stack */
   k_render_batch<BS, kNee, kFast>
-      <<<persistent_grid(k_render_batch<BS, kNee, kFast>, BS, b->total_tiles * 32, smem), BS, smem, st>>>(
+      <<<persistent_grid(k_render_batch<BS, kNee, kFast>, BS, b->total_tiles * 32), BS, 0, st>>>(
           b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
 }
 

@@ -42,54 +42,13 @@
  * are held to the north star's statistical bar (per-channel relative RMSE
  * and mean luminance against the oracle), not to bit equality.
  *
- * Stack entries are 8 bytes (packed payload word + float entry distance;
- * the any-hit walk uses the word only), the top ones in shared memory.
+ * Stack entries are 8 bytes (packed payload word + float entry distance),
+ * 4 bytes in the any-hit walk.
  */
 #ifndef ZT_FAST_CUH
 #define ZT_FAST_CUH
 
 namespace zt {
-
-/* Short traversal stack: the top kFastSharedEntries entries of each
- * thread's stack live in dynamic shared memory, entry i of thread t at
- * [i * blockDim.x + t] (a warp touching the same depth hits 32 consecutive
- * 8-byte words), deeper entries in a per-thread local array.  Stacks rarely
- * grow past a few entries, so the walk's pushes and pops stay on chip
- * instead of going through L1 to L2 as local memory.  Kernels that use the
- * fast walk are launched with fast_stack_bytes(block size) of dynamic shared
- * memory and check it on entry (fast_stack_ok). */
-#ifndef ZT_FAST_SHARED_ENTRIES
-#define ZT_FAST_SHARED_ENTRIES 8
-#endif
-constexpr int kFastSharedEntries = ZT_FAST_SHARED_ENTRIES;
-
-__host__ __device__ constexpr size_t fast_stack_bytes(int block) {
-  return (size_t)kFastSharedEntries * (size_t)block * sizeof(uint2);
-}
-
-ZT_D uint2* fast_stack_smem() {
-  extern __shared__ uint2 zt_fast_stack_smem[];
-  return zt_fast_stack_smem;
-}
-
-/* Whether this launch has the dynamic shared memory the stack needs. */
-ZT_D bool fast_stack_ok() {
-  uint32_t dyn;
-  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-  return (size_t)dyn >= fast_stack_bytes(blockDim.x);
-}
-
-struct FastStack {
-  uint2* sm;                                    /* this thread's column */
-  uint32_t stride;
-  uint2 lm[kStackSize - kFastSharedEntries];   /* deeper entries */
-  ZT_D FastStack() : sm(fast_stack_smem() + threadIdx.x), stride(blockDim.x) {}
-  ZT_D void put(int i, uint2 v) {
-    if (i < kFastSharedEntries) sm[(uint32_t)i * stride] = v;
-    else lm[i - kFastSharedEntries] = v;
-  }
-  ZT_D uint2 get(int i) const { return i < kFastSharedEntries ? sm[(uint32_t)i * stride] : lm[i - kFastSharedEntries]; }
-};
 
 /* Per-ray constants of the float slab test. */
 struct FRay {
@@ -182,7 +141,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
     float t;
     if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
               tmin32, cl32, t)) {
-      FastStack stack; /* (payload word, entry distance bits) */
+      uint2 stack[kStackSize]; /* (payload word, entry distance bits) */
       uint32_t w = sc.froot_word;
       float et = t;
       bool have = true;
@@ -190,7 +149,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
       for (;;) {
         if (!have) {
           if (sp == 0) break;
-          const uint2 e = stack.get(--sp);
+          const uint2 e = stack[--sp];
           w = e.x;
           et = __uint_as_float(e.y);
         }
@@ -214,7 +173,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
         const bool hr = fslab_right(r, fr, tmin32, cl32, tr);
         if (hl && hr) { /* push the farther child; the nearer one is next */
           const bool near_left = tl <= tr;
-          stack.put(sp, make_uint2(near_left ? r.w.y : r.w.x, __float_as_uint(near_left ? tr : tl)));
+          stack[sp] = make_uint2(near_left ? r.w.y : r.w.x, __float_as_uint(near_left ? tr : tl));
           sp += 1;
           w = near_left ? r.w.x : r.w.y;
           et = near_left ? tl : tr;
@@ -250,14 +209,14 @@ ZT_D bool scene_occluded_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
     float t;
     if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
               tmin32, tmax32, t)) {
-      FastStack stack;
+      uint32_t stack[kStackSize];
       uint32_t w = sc.froot_word;
       bool have = true;
       int sp = 0;
       for (;;) {
         if (!have) {
           if (sp == 0) break;
-          w = stack.get(--sp).x;
+          w = stack[--sp];
         }
         have = false;
         const uint32_t cnt = w >> kFastCountShift, first = w & kFastFirstMask;
@@ -274,7 +233,7 @@ ZT_D bool scene_occluded_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
         const bool hr = fslab_right(r, fr, tmin32, tmax32, tr);
         if (hl && hr) {
           const bool left_first = tl > tr; /* the farther child first */
-          stack.put(sp++, make_uint2(left_first ? r.w.y : r.w.x, 0u));
+          stack[sp++] = left_first ? r.w.y : r.w.x;
           w = left_first ? r.w.x : r.w.y;
           have = true;
         } else if (hl || hr) {

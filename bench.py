@@ -319,7 +319,7 @@ def b200_arm(args):
     if args.autotune:  # mode, block size and queue capacity from the project's autotuner
         from zigtrace_b200 import autotune
         gcfg, tune_ms, tune_cached = autotune.tune_render(scene, o, reps=1, precision=prec)
-        tuned = {"mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][gcfg.mode],
+        tuned = {"mode": ["auto", "megakernel", "wavefront", "megakernel_regen", "wavefront_sorted"][gcfg.mode],
                  "block_size": gcfg.block_size, "queue_capacity": gcfg.queue_capacity, "precision": args.precision,
                  "cached": tune_cached, "candidates_ms": tune_ms,
                  "candidate_key": "[mode, block_size, queue_capacity]"}
@@ -438,7 +438,7 @@ def b200_arm(args):
              if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and gcfg.mode in (0, 1) else None),
             "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
             NCU_EXECUTION.get(args.workload) if gcfg.mode in (0, 1) else None)
-        if gcfg.mode == 2:  # the wavefront form: path-state traffic through HBM against the copy peak
+        if gcfg.mode in (2, 4):  # the wavefront form: path-state traffic through HBM against the copy peak
             qbps = queue_bytes * samples / (kernel_ms / 1e3) / 1e9
             roofline["queue"] = {"bytes_per_sample": round(queue_bytes, 1), "achieved_gbs": round(qbps, 1),
                                  "peak_gbs": roofline["memory"]["peak_gbs"],
@@ -451,7 +451,7 @@ def b200_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {**describe(args.workload, scene, o, counts), "l2": "flushed by a 256 MB write before every step",
-                   "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][gcfg.mode],
+                   "mode": ["auto", "megakernel", "wavefront", "megakernel_regen", "wavefront_sorted"][gcfg.mode],
                    "precision": args.precision, "autotune": tuned,
                    "sharding": "one frame per rank (seed = rank), no collective",
                    "bvh_build": {"on_device": scene.built_on_device,

@@ -84,8 +84,11 @@ typedef struct { zt_shape shape; zt_vec3 radiance; double weight; } zt_light;
  * (a lane whose path ends starts its next sample at once); faster on closed
  * scenes with long paths.  AUTO is MEGAKERNEL_REGEN when the mean path
  * length of a 64x64, 1-spp pilot traced at zt_scene_upload is at least 3,
- * else MEGAKERNEL.  All modes give bit-identical images. */
-enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_MEGAKERNEL_REGEN = 3 };
+ * else MEGAKERNEL.  WAVEFRONT_SORTED: the wavefront form with its extension
+ * queue sorted between bounces by ray direction octant and origin cell.
+ * All modes give bit-identical images. */
+enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_MEGAKERNEL_REGEN = 3,
+       ZT_MODE_WAVEFRONT_SORTED = 4 };
 /* ZT_PRECISION_EXACT (the default) is the verification build of the path:
  * every operation is the reference's f64 operation in the reference's order,
  * so images are bit-identical to the reference algorithm's.

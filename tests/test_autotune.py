@@ -26,7 +26,7 @@ def test_choose_picks_fastest_and_caches(tmp_path, monkeypatch):
 
 def test_candidates_cover_modes_blocks_and_queue_capacities():
     modes = {m for m, _, _ in autotune.SINGLE_CANDIDATES}
-    assert modes == {zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN, zt.MODE_WAVEFRONT}
+    assert modes == {zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN, zt.MODE_WAVEFRONT, zt.MODE_WAVEFRONT_SORTED}
     caps = {c for m, _, c in autotune.SINGLE_CANDIDATES if m == zt.MODE_WAVEFRONT}
     assert len(caps) >= 3 and 0 in caps
     assert {b for m, b, _ in autotune.SINGLE_CANDIDATES if m == zt.MODE_MEGAKERNEL} == {64, 128, 256}

@@ -17,7 +17,7 @@ from zigtrace_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 MODES = [pytest.param(zt.MODE_MEGAKERNEL, id="mega"), pytest.param(zt.MODE_WAVEFRONT, id="wavefront"),
-         pytest.param(zt.MODE_MEGAKERNEL_REGEN, id="regen")]
+         pytest.param(zt.MODE_MEGAKERNEL_REGEN, id="regen"), pytest.param(zt.MODE_WAVEFRONT_SORTED, id="wf_sorted")]
 
 DEBUG_CASES = {
     "demo": (K.demo_scene, dict(width=48, height=32, max_depth=8)),

@@ -21,7 +21,8 @@ def _as_abi(nodes):
     return out
 
 
-@pytest.mark.parametrize("mode", [zt.MODE_MEGAKERNEL, zt.MODE_WAVEFRONT, zt.MODE_MEGAKERNEL_REGEN])
+@pytest.mark.parametrize("mode", [zt.MODE_MEGAKERNEL, zt.MODE_WAVEFRONT, zt.MODE_MEGAKERNEL_REGEN,
+                                  zt.MODE_WAVEFRONT_SORTED])
 @pytest.mark.parametrize("make,o", [(scenes.cornell, zt.Options(64, 64, 4, 16)),
                                     (lambda: K.fuzz_scene(5), zt.Options(48, 32, 8, 12, seed=5))])
 def test_imported_tree_renders_bit_exact(make, o, mode):

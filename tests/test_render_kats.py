@@ -13,7 +13,8 @@ import zigtrace_b200 as zt
 BACKENDS = [pytest.param(OracleBackend(), id="oracle"),
             pytest.param(GpuBackend(zt.MODE_MEGAKERNEL), id="gpu-mega", marks=pytest.mark.gpu),
             pytest.param(GpuBackend(zt.MODE_WAVEFRONT), id="gpu-wavefront", marks=pytest.mark.gpu),
-            pytest.param(GpuBackend(zt.MODE_MEGAKERNEL_REGEN), id="gpu-regen", marks=pytest.mark.gpu)]
+            pytest.param(GpuBackend(zt.MODE_MEGAKERNEL_REGEN), id="gpu-regen", marks=pytest.mark.gpu),
+            pytest.param(GpuBackend(zt.MODE_WAVEFRONT_SORTED), id="gpu-wf-sorted", marks=pytest.mark.gpu)]
 
 
 @pytest.mark.parametrize("be", BACKENDS)

@@ -10,7 +10,7 @@ radiance path, behind a mirror of the reference library API.
     rgb = img.to_rgb8(zt.Output(tonemap="aces"))
 """
 from .api import (  # noqa: F401
-    DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, PLANE, PRECISION_EXACT, PRECISION_FAST, SPHERE, TRIANGLE,
+    DIELECTRIC, EMISSIVE, LAMBERTIAN, METAL, MODE_AUTO, MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, MODE_WAVEFRONT_SORTED, PLANE, PRECISION_EXACT, PRECISION_FAST, SPHERE, TRIANGLE,
     Background, Batch, CameraConfig, GpuConfig, Image, Material, Options, Output, Scene, Settings, ZigtraceError,
     backward, backward_rows, encode_png, encode_png_device, forward, forward_rows, image_to_rgb8_device, plane, png_size, render, render_batch,
     render_debug, render_device, render_function, render_rows_device, render_png, render_rgb8, rng_streams, set_colors, sphere, triangle,

@@ -23,7 +23,7 @@ Vec = Sequence[float]
 
 LAMBERTIAN, METAL, DIELECTRIC, EMISSIVE = 0, 1, 2, 3
 SPHERE, TRIANGLE, PLANE = 0, 1, 2
-MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, MODE_MEGAKERNEL_REGEN = 0, 1, 2, 3
+MODE_AUTO, MODE_MEGAKERNEL, MODE_WAVEFRONT, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT_SORTED = 0, 1, 2, 3, 4
 PRECISION_EXACT, PRECISION_FAST = 0, 1
 
 

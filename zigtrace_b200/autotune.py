@@ -1,9 +1,9 @@
 """Autotuner for the device execution choices.
 
 For a render it times the megakernel at block sizes 64/128/256, the
-megakernel with path regeneration at 128/256, and the wavefront form at
-three queue capacities (paths in flight: the default of one slot per pixel
-up to 4M, 1M and 256K).  For a batch it times the batched persistent launch
+megakernel with path regeneration at 128/256, the wavefront form at three
+queue capacities (paths in flight: the default of one slot per pixel up to
+4M, 1M and 256K) and the sorted wavefront form at two.  For a batch it times the batched persistent launch
 at block sizes 64/128/256 with the renders in the given order or largest
 first, and the same renders as plain per-render launches (each with its own
 default choice) as one more candidate.  Every candidate renders identical
@@ -23,12 +23,13 @@ import statistics
 from pathlib import Path
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
-from .api import MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, Batch, GpuConfig, Options, Scene, render_device
+from .api import MODE_MEGAKERNEL, MODE_MEGAKERNEL_REGEN, MODE_WAVEFRONT, MODE_WAVEFRONT_SORTED, Batch, GpuConfig, Options, Scene, render_device
 
 SINGLE_CANDIDATES: List[Tuple[int, int, int]] = [  # (mode, block_size, queue_capacity)
     (MODE_MEGAKERNEL, 64, 0), (MODE_MEGAKERNEL, 128, 0), (MODE_MEGAKERNEL, 256, 0),
     (MODE_MEGAKERNEL_REGEN, 128, 0), (MODE_MEGAKERNEL_REGEN, 256, 0),
-    (MODE_WAVEFRONT, 128, 0), (MODE_WAVEFRONT, 128, 1 << 20), (MODE_WAVEFRONT, 128, 1 << 18)]
+    (MODE_WAVEFRONT, 128, 0), (MODE_WAVEFRONT, 128, 1 << 20), (MODE_WAVEFRONT, 128, 1 << 18),
+    (MODE_WAVEFRONT_SORTED, 128, 0), (MODE_WAVEFRONT_SORTED, 128, 1 << 20)]
 PLAIN = -1  # batch candidate: plain per-render launches instead of the batched launch
 BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)] + [(PLAIN, 0)]
 

@@ -11,6 +11,7 @@
  */
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -683,6 +684,120 @@ __global__ void __launch_bounds__(128) k_wf_shadow(DevScene sc, RenderParams p, 
   }
 }
 
+/* Queue sort, step 1: the bucket of every entry of the next extension queue
+ * (direction octant, Morton cell of the origin) and per-bucket counts (a
+ * shared-memory histogram per block, added to the global counts). */
+__global__ void __launch_bounds__(256) k_wf_sort_keys(DevScene sc, WfState w) {
+  __shared__ uint32_t hist[kSortBuckets];
+  for (uint32_t i = threadIdx.x; i < kSortBuckets; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const uint32_t nxt = (w.ctl[kCtlIter] & 1) ^ 1;
+  const uint32_t n = w.ctl[kCtlExt0 + nxt];
+  const uint32_t* __restrict__ q = w.queue[nxt];
+  const uint32_t c = w.capacity;
+  const double cells = (double)(1u << kSortCellBits);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = q[i];
+    const dv3 o = ld3(w.ray, c, s, 0), d = ld3(w.ray, c, s, 3);
+    const uint32_t oct = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    uint32_t cell[3];
+    const double oo[3] = {o.x, o.y, o.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double ext = sc.root_hi[a] - sc.root_lo[a];
+      const double f = ext > 0 ? (oo[a] - sc.root_lo[a]) / ext * cells : 0.0;
+      cell[a] = f >= cells ? (1u << kSortCellBits) - 1 : (f > 0 ? (uint32_t)f : 0u); /* NaN -> 0 */
+    }
+    uint32_t morton = 0;
+#pragma unroll
+    for (uint32_t b = 0; b < kSortCellBits; ++b)
+      morton |= (((cell[0] >> b) & 1u) << (3 * b)) | (((cell[1] >> b) & 1u) << (3 * b + 1)) |
+                (((cell[2] >> b) & 1u) << (3 * b + 2));
+    const uint32_t key = (oct << (3 * kSortCellBits)) | morton;
+    w.sort_key[i] = key;
+    atomicAdd(&hist[key], 1u);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < kSortBuckets; i += blockDim.x)
+    if (hist[i]) atomicAdd(&w.sort_hist[i], hist[i]);
+}
+
+/* Step 2: counts -> exclusive offsets (one block of 1024 threads, 4 buckets
+ * per thread). */
+__global__ void __launch_bounds__(1024) k_wf_sort_scan(WfState w) {
+  __shared__ uint32_t part[1024];
+  constexpr uint32_t per = kSortBuckets / 1024;
+  uint32_t v[per], sum = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < per; ++k) {
+    v[k] = w.sort_hist[threadIdx.x * per + k];
+    sum += v[k];
+  }
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) { /* inclusive scan of the per-thread sums */
+    const uint32_t add = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += add;
+    __syncthreads();
+  }
+  uint32_t run = part[threadIdx.x] - sum;
+#pragma unroll
+  for (uint32_t k = 0; k < per; ++k) {
+    w.sort_hist[threadIdx.x * per + k] = run;
+    run += v[k];
+  }
+}
+
+/* Step 3: every entry to its place (warp-aggregated per bucket); the order
+ * within a bucket is arbitrary, which changes nothing: paths are
+ * independent and each pixel belongs to one slot at a time. */
+__global__ void __launch_bounds__(256) k_wf_sort_scatter(WfState w) {
+  const uint32_t nxt = (w.ctl[kCtlIter] & 1) ^ 1;
+  const uint32_t n = w.ctl[kCtlExt0 + nxt];
+  const uint32_t* __restrict__ q = w.queue[nxt];
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    const bool live = i < n;
+    const uint32_t key = live ? w.sort_key[i] : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (live) {
+      const int leader = __ffs(peers) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(&w.sort_hist[key], (uint32_t)__popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      w.sort_tmp[base + __popc(peers & ((1u << lane) - 1))] = q[i];
+    }
+  }
+}
+
+/* Step 4: the sorted queue back in place; counts cleared for the next sort. */
+__global__ void __launch_bounds__(256) k_wf_sort_copy(WfState w) {
+  const uint32_t nxt = (w.ctl[kCtlIter] & 1) ^ 1;
+  const uint32_t n = w.ctl[kCtlExt0 + nxt];
+  uint32_t* q = w.queue[nxt];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) q[i] = w.sort_tmp[i];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kSortBuckets; i += gridDim.x * blockDim.x)
+    w.sort_hist[i] = 0;
+}
+
+/* k_wf_advance for the host-driven loop: the condition goes to ctl[kCtlGo]. */
+__global__ void k_wf_advance_host(WfState w, uint64_t max_iter) {
+  const uint32_t it = w.ctl[kCtlIter];
+  const uint32_t nxt = (it & 1) ^ 1;
+  const uint32_t n_next = w.ctl[kCtlExt0 + nxt];
+  w.ctl[kCtlExt0 + (it & 1)] = 0;
+  w.ctl[kCtlShadow] = 0;
+  w.ctl[kCtlIter] = it + 1;
+  bool go = n_next > 0;
+  if (go && (uint64_t)it + 1 >= max_iter) {
+    w.ctl[kCtlError] = 1;
+    go = false;
+  }
+  w.ctl[kCtlGo] = go ? 1u : 0u;
+}
+
 /* Swaps the queues and sets the while-node condition.  The loop provably
  * ends (every active slot advances one bounce per iteration); max_iter is a
  * guard that reports an error instead of looping. */
@@ -808,9 +923,9 @@ static zt_status wavefront_state(zt_device_buffers* d, uint32_t cap) {
   c.capacity = 0;
   const size_t n = cap;
   const size_t sizes[] = {4 * n, 4 * n, 4 * n, 4 * n, 32 * n, 48 * n, 24 * n, 24 * n, 24 * n, 32 * n,
-                          8 * n, 4 * n, 104 * n, 4 * n, 4 * n, 4 * n, 64};
-  size_t offs[17], cur = 0;
-  for (int i = 0; i < 17; ++i) { offs[i] = cur; cur = align256(cur + sizes[i]); }
+                          8 * n, 4 * n, 104 * n, 4 * n, 4 * n, 4 * n, 64, 4 * n, 4 * n, 4 * kSortBuckets};
+  size_t offs[20], cur = 0;
+  for (int i = 0; i < 20; ++i) { offs[i] = cur; cur = align256(cur + sizes[i]); }
   ZT_CUDA(cudaMalloc(&c.block, cur), "allocate wavefront state");
   char* b = (char*)c.block;
   WfState& w = c.state;
@@ -831,6 +946,10 @@ static zt_status wavefront_state(zt_device_buffers* d, uint32_t cap) {
   w.queue[1] = (uint32_t*)(b + offs[14]);
   w.shadow_q = (uint32_t*)(b + offs[15]);
   w.ctl = (uint32_t*)(b + offs[16]);
+  w.sort_key = (uint32_t*)(b + offs[17]);
+  w.sort_tmp = (uint32_t*)(b + offs[18]);
+  w.sort_hist = (uint32_t*)(b + offs[19]);
+  ZT_CUDA(cudaMemset(w.sort_hist, 0, 4 * kSortBuckets), "clear the queue sort's counts");
   w.capacity = cap;
   c.bytes = cur;
   c.capacity = cap;
@@ -839,8 +958,24 @@ static zt_status wavefront_state(zt_device_buffers* d, uint32_t cap) {
 
 /* Builds the executable graph: while (queue not empty) { extend; shade;
  * shadow; advance }.  The loop runs on the device; the host never waits. */
+/* One iteration's kernels after the intersection: shade, shadow and, for
+ * the sorted form, the four queue-sort kernels. */
+static void enqueue_wavefront_step(const DevScene& view, const RenderParams& p, const WfState& w, double* d_out,
+                                   bool sorted, cudaStream_t cs) {
+  const uint64_t cap = w.capacity;
+  k_wf_extend<<<persistent_grid(k_wf_extend, 128, cap), 128, 0, cs>>>(view, w);
+  k_wf_shade<<<persistent_grid(k_wf_shade, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
+  k_wf_shadow<<<persistent_grid(k_wf_shadow, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
+  if (sorted) {
+    k_wf_sort_keys<<<persistent_grid(k_wf_sort_keys, 256, cap), 256, 0, cs>>>(view, w);
+    k_wf_sort_scan<<<1, 1024, 0, cs>>>(w);
+    k_wf_sort_scatter<<<persistent_grid(k_wf_sort_scatter, 256, cap), 256, 0, cs>>>(w);
+    k_wf_sort_copy<<<persistent_grid(k_wf_sort_copy, 256, cap), 256, 0, cs>>>(w);
+  }
+}
+
 static zt_status build_wavefront_graph(const DevScene& view, const RenderParams& p, const WfState& w, double* d_out,
-                                       uint64_t max_iter, cudaGraphExec_t* exec_out) {
+                                       uint64_t max_iter, bool sorted, cudaGraphExec_t* exec_out) {
   cudaGraph_t g = nullptr;
   cudaStream_t cs = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -858,10 +993,7 @@ static zt_status build_wavefront_graph(const DevScene& view, const RenderParams&
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      const uint64_t cap = w.capacity;
-      k_wf_extend<<<persistent_grid(k_wf_extend, 128, cap), 128, 0, cs>>>(view, w);
-      k_wf_shade<<<persistent_grid(k_wf_shade, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
-      k_wf_shadow<<<persistent_grid(k_wf_shadow, 128, cap), 128, 0, cs>>>(view, p, w, d_out);
+      enqueue_wavefront_step(view, p, w, d_out, sorted, cs);
       k_wf_advance<<<1, 1, 0, cs>>>(w, h, max_iter);
       cudaGraph_t captured = nullptr;
       cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
@@ -890,7 +1022,23 @@ static uint64_t wavefront_max_iter(const RenderParams& p) {
   return max_iter;
 }
 
-static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t capacity, double* d_out,
+/* The same loop driven from the host, one synchronisation per iteration,
+ * when ZT_WAVEFRONT_HOST_LOOP is set in the environment: profilers that do
+ * not see kernels inside a conditional graph node can then measure the
+ * wavefront kernels one launch at a time.  Same kernels, same pixels. */
+static zt_status run_wavefront_host_loop(const DevScene& view, const RenderParams& p, const WfState& w,
+                                         double* d_out, uint64_t max_iter, bool sorted, cudaStream_t stream) {
+  for (;;) {
+    enqueue_wavefront_step(view, p, w, d_out, sorted, stream);
+    k_wf_advance_host<<<1, 1, 0, stream>>>(w, max_iter);
+    uint32_t go = 0;
+    ZT_CUDA(cudaMemcpyAsync(&go, w.ctl + kCtlGo, sizeof go, cudaMemcpyDeviceToHost, stream), "read loop condition");
+    ZT_CUDA(cudaStreamSynchronize(stream), "wavefront iteration");
+    if (!go) return ZT_OK;
+  }
+}
+
+static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t capacity, bool sorted, double* d_out,
                                   cudaStream_t stream) {
   zt_device_buffers* d = s->device;
   const uint64_t npix = p.width * p.height;
@@ -904,18 +1052,23 @@ static zt_status launch_wavefront(zt_scene* s, const RenderParams& p, uint32_t c
   memcpy(key, &view, sizeof view);
   memcpy(key + sizeof view, &p, sizeof p);
   memcpy(key + sizeof view + sizeof p, &d_out, sizeof d_out);
-  const uint64_t capk = cap, max_iter = wavefront_max_iter(p);
+  const uint64_t capk = cap | (sorted ? 1ull << 40 : 0ull), max_iter = wavefront_max_iter(p);
   memcpy(key + sizeof view + sizeof p + sizeof d_out, &capk, sizeof capk);
   memcpy(key + sizeof view + sizeof p + sizeof d_out + sizeof capk, &max_iter, sizeof max_iter);
+  const uint32_t n0 = (uint32_t)(npix < cap ? npix : cap);
+  if (getenv("ZT_WAVEFRONT_HOST_LOOP")) {
+    k_wf_init<<<persistent_grid(k_wf_init, 256, n0), 256, 0, stream>>>(p, c.state, n0);
+    ZT_CUDA(cudaGetLastError(), "launch k_wf_init");
+    return run_wavefront_host_loop(view, p, c.state, d_out, max_iter, sorted, stream);
+  }
   if (!c.exec || memcmp(key, c.key, sizeof key) != 0) {
     if (c.done) cudaEventSynchronize(c.done);
     if (c.exec) { cudaGraphExecDestroy(c.exec); c.exec = nullptr; }
-    rc = build_wavefront_graph(view, p, c.state, d_out, max_iter, &c.exec);
+    rc = build_wavefront_graph(view, p, c.state, d_out, max_iter, sorted, &c.exec);
     if (rc != ZT_OK) return rc;
     memcpy(c.key, key, sizeof key);
     if (!c.done) ZT_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "create event");
   }
-  const uint32_t n0 = (uint32_t)(npix < cap ? npix : cap);
   k_wf_init<<<persistent_grid(k_wf_init, 256, n0), 256, 0, stream>>>(p, c.state, n0);
   ZT_CUDA(cudaGetLastError(), "launch k_wf_init");
   ZT_CUDA(cudaGraphLaunch(c.exec, stream), "launch wavefront graph");
@@ -932,10 +1085,10 @@ static zt_status launch_render_params(zt_scene* s, const RenderParams& p, const 
     return ZT_OK;
   }
   const uint32_t mode = cfg ? cfg->mode : ZT_MODE_AUTO;
-  if (mode == ZT_MODE_WAVEFRONT) {
+  if (mode == ZT_MODE_WAVEFRONT || mode == ZT_MODE_WAVEFRONT_SORTED) {
     if (p.row0 != 0 || p.rows != p.height)
       return fail(ZT_ERR_INVALID_ARGUMENT, "the wavefront mode renders whole images, not row bands");
-    return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, d_out, stream);
+    return launch_wavefront(s, p, cfg ? cfg->queue_capacity : 0, mode == ZT_MODE_WAVEFRONT_SORTED, d_out, stream);
   }
   if (mode > ZT_MODE_MEGAKERNEL_REGEN) return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.mode");
   const uint32_t bs = cfg ? cfg->block_size : 0;
@@ -955,7 +1108,9 @@ static zt_status launch_render(zt_scene* s, const zt_options* o, const zt_gpu_co
 
 /* Error word of the last wavefront launch (after the stream is idle). */
 static zt_status wavefront_status(zt_scene* s, const zt_gpu_config* cfg) {
-  if (!cfg || cfg->mode != ZT_MODE_WAVEFRONT || !s->device || !s->device->wf.block) return ZT_OK;
+  if (!cfg || (cfg->mode != ZT_MODE_WAVEFRONT && cfg->mode != ZT_MODE_WAVEFRONT_SORTED) || !s->device ||
+      !s->device->wf.block)
+    return ZT_OK;
   uint32_t err = 0;
   ZT_CUDA(cudaMemcpy(&err, s->device->wf.state.ctl + kCtlError, sizeof err, cudaMemcpyDeviceToHost), "read status");
   if (err) return fail(ZT_ERR_TIMEOUT, "wavefront loop exceeded its iteration bound");

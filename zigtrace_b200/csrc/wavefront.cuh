@@ -41,11 +41,21 @@ struct WfState {
   double* nee;        /* shadow ray o.xyz d.xyz tmax, contribution.xyz, throughput.xyz: 13 per slot */
   uint32_t* queue[2]; /* ping-pong extension queues */
   uint32_t* shadow_q; /* slots with a pending light sample */
-  uint32_t* ctl;      /* [0] iter, [1] n_ext[0], [2] n_ext[1], [3] n_shadow, [4] next pixel, [5] error */
+  uint32_t* ctl;      /* [0] iter, [1] n_ext[0], [2] n_ext[1], [3] n_shadow, [4] next pixel, [5] error, [6] go */
+  uint32_t* sort_key; /* queue sort: bucket of each queue entry */
+  uint32_t* sort_tmp; /* queue sort: the sorted queue before it is copied back */
+  uint32_t* sort_hist;/* queue sort: kSortBuckets counts, then running offsets */
   uint32_t capacity;
 };
 
-enum { kCtlIter = 0, kCtlExt0 = 1, kCtlShadow = 3, kCtlNextPixel = 4, kCtlError = 5 };
+enum { kCtlIter = 0, kCtlExt0 = 1, kCtlShadow = 3, kCtlNextPixel = 4, kCtlError = 5, kCtlGo = 6 };
+
+/* Extension rays are sorted between iterations by direction octant (3 bits)
+ * and the cell of their origin on an 8x8x8 grid over the scene bounds
+ * (9 bits, Morton order): rays in one warp then start near one another and
+ * head the same way, so they walk more of the same BVH nodes together. */
+constexpr uint32_t kSortCellBits = 3;
+constexpr uint32_t kSortBuckets = 8u << (3 * kSortCellBits);
 
 ZT_D dv3 ld3(const double* a, uint32_t cap, uint32_t s, int c0) {
   return V(a[(size_t)c0 * cap + s], a[(size_t)(c0 + 1) * cap + s], a[(size_t)(c0 + 2) * cap + s]);

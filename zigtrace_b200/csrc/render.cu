@@ -328,10 +328,14 @@ constexpr int kMegaThreadsPerSmNoNee = 896;
 #ifndef ZT_FAST_THREADS_PER_SM
 #define ZT_FAST_THREADS_PER_SM 896
 #endif
+#ifndef ZT_FAST_THREADS_PER_SM_NONEE
+#define ZT_FAST_THREADS_PER_SM_NONEE 896
+#endif
 /* Resident threads per SM each megakernel and batch instance is built for
  * (__launch_bounds__): sets the register budget, 65,536 / threads. */
 __host__ __device__ constexpr int mega_threads_per_sm(bool nee, bool fast) {
-  return fast ? ZT_FAST_THREADS_PER_SM : (nee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee);
+  return fast ? (nee ? ZT_FAST_THREADS_PER_SM : ZT_FAST_THREADS_PER_SM_NONEE)
+              : (nee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee);
 }
 
 template <int BS, bool kNee, bool kFast = false>
@@ -460,16 +464,13 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_render_regen(DevScene sc, Rend
 
 /* One render of a batch: its scene view, parameters, output and the index
  * of its first tile in the batch-wide tile numbering. */
-struct __align__(16) BatchItem {
+struct BatchItem {
   DevScene sc;
   RenderParams p;
   double* out;
   uint64_t tile_begin;
   uint64_t tiles_x;
 };
-#ifndef ZT_BATCH_STAGE_ITEM
-#define ZT_BATCH_STAGE_ITEM 0
-#endif
 
 /* Batched persistent launch: many renders of uneven size share one grid.
  * Warps take 8x4 tiles from one counter over the concatenated tile ranges of
@@ -482,10 +483,6 @@ __global__ void __launch_bounds__(BS, mega_threads_per_sm(kNee, kFast) / BS)
     k_render_batch(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
                    unsigned int* __restrict__ counter) {
   const unsigned lane = threadIdx.x & 31;
-#if ZT_BATCH_STAGE_ITEM
-  __shared__ __align__(16) BatchItem s_items[BS / 32];
-  uint32_t cur_item = 0xFFFFFFFFu;
-#endif
   for (;;) {
     unsigned tile = 0;
     if (lane == 0) tile = atomicAdd(counter, 1u);
@@ -497,22 +494,7 @@ __global__ void __launch_bounds__(BS, mega_threads_per_sm(kNee, kFast) / BS)
       if (items[mid].tile_begin <= tile) lo = mid;
       else hi = mid - 1;
     }
-#if ZT_BATCH_STAGE_ITEM
-    /* the warp's render, copied into shared memory when it changes: its
-     * scene view and parameters are read on every traversal step, and a
-     * shared copy keeps them out of L1's way */
-    BatchItem& it = s_items[threadIdx.x >> 5];
-    if (lo != cur_item) {
-      __syncwarp();
-      const uint4* src = reinterpret_cast<const uint4*>(items + lo);
-      uint4* dst = reinterpret_cast<uint4*>(&it);
-      for (uint32_t k = lane; k < sizeof(BatchItem) / sizeof(uint4); k += 32) dst[k] = __ldg(src + k);
-      __syncwarp();
-      cur_item = lo;
-    }
-#else
     const BatchItem& it = items[lo];
-#endif
     const uint64_t local = tile - it.tile_begin;
     const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
     if (x < it.p.width && y < it.p.height)

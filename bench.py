@@ -573,8 +573,8 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
     cfg, order, tune_ms, cached = autotune.tune_batch(scs, opts, reps=1, precision=prec)
     plain_won = order == autotune.PLAIN
     if plain_won:  # still measure the best batched launch against the plain launches
-        best = min((k for k in tune_ms if json.loads(k)[0] != autotune.PLAIN), key=tune_ms.get)
-        cfg, order = zt.GpuConfig(block_size=json.loads(best)[0], precision=prec), json.loads(best)[1]
+        best = json.loads(min((k for k in tune_ms if json.loads(k)[0] != autotune.PLAIN), key=tune_ms.get))
+        cfg, order = zt.GpuConfig(mode=best[2], block_size=best[0], precision=prec), best[1]
     batch = zt.Batch(scs, opts, [t.data_ptr() for t in outs], cfg, order)
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -695,8 +695,9 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
                    "l2": "flushed by a 256 MB write before every step",
                    "precision": args.precision,
                    "autotune": {"block_size": cfg.block_size, "order": ["given", "largest_first"][order],
+                                "mode": ["auto", "megakernel", "wavefront", "megakernel_regen"][cfg.mode],
                                 "plain_launches_won": plain_won, "cached": cached, "candidates_ms": tune_ms,
-                                "candidate_key": "[block_size, order]; [-1, 0] = plain per-render launches"},
+                                "candidate_key": "[block_size, order, mode]; [-1, 0, 1] = plain per-render launches"},
                    "sharding": "one batch per rank (seeds offset by rank), no collective"},
         "plain_launches": {"value": round(plain_value, 4), "unit": "Msamples/s", "ms_per_step": round(plain_ms, 3),
                            "launches_per_step": len(items)},

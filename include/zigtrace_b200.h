@@ -249,7 +249,10 @@ zt_status zt_backward_rows(zt_scene* scene, const zt_options* opts, uint64_t row
  * and those options.  order: 0 = tiles in the given order, 1 = largest
  * renders first.  Scenes are uploaded to the current device if needed.  The
  * batch keeps pointers to the scenes' device copies: destroy it before the
- * scenes change or are destroyed.  block_size in cfg: 0/64/128/256. */
+ * scenes change or are destroyed.  block_size in cfg: 0/64/128/256; mode:
+ * ZT_MODE_AUTO or ZT_MODE_MEGAKERNEL (the nested megakernel) or
+ * ZT_MODE_MEGAKERNEL_REGEN (per-lane path regeneration); precision as for a
+ * single render. */
 typedef struct zt_batch zt_batch;
 zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint64_t n, double* const* d_outs,
                           const zt_gpu_config* cfg, uint32_t order, zt_batch** out);

@@ -30,8 +30,9 @@ def test_candidates_cover_modes_blocks_and_queue_capacities():
     caps = {c for m, _, c in autotune.SINGLE_CANDIDATES if m == zt.MODE_WAVEFRONT}
     assert len(caps) >= 3 and 0 in caps
     assert {b for m, b, _ in autotune.SINGLE_CANDIDATES if m == zt.MODE_MEGAKERNEL} == {64, 128, 256}
-    assert (autotune.PLAIN, 0) in autotune.BATCH_CANDIDATES
-    assert {o for b, o in autotune.BATCH_CANDIDATES if b != autotune.PLAIN} == {0, 1}
+    assert (autotune.PLAIN, 0, zt.MODE_MEGAKERNEL) in autotune.BATCH_CANDIDATES
+    assert {o for b, o, _ in autotune.BATCH_CANDIDATES if b != autotune.PLAIN} == {0, 1}
+    assert {m for _, _, m in autotune.BATCH_CANDIDATES} == {zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN}
 
 
 def test_scene_class_keys(native_lib):

@@ -33,15 +33,16 @@ def test_render_batch_equals_single_renders():
                                                                          seed=o.seed).tobytes()
 
 
+@pytest.mark.parametrize("mode", [zt.MODE_MEGAKERNEL, zt.MODE_MEGAKERNEL_REGEN])
 @pytest.mark.parametrize("block_size", [64, 128, 256])
 @pytest.mark.parametrize("order", [0, 1])
-def test_batch_object_all_configs_and_replay(block_size, order):
+def test_batch_object_all_configs_and_replay(block_size, order, mode):
     import torch
     items = mixed_batch()
     want = [zt.render(s, o).pixels for s, o in items]
     outs = [torch.full((o.width * o.height * 3,), -1.0, dtype=torch.float64, device="cuda") for _, o in items]
     b = zt.Batch([s for s, _ in items], [o for _, o in items], [t.data_ptr() for t in outs],
-                 zt.GpuConfig(block_size=block_size), order=order)
+                 zt.GpuConfig(mode=mode, block_size=block_size), order=order)
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(2):  # replay the captured graph
         for t in outs:
@@ -70,6 +71,9 @@ def test_autotuned_configs_render_identical_pixels(tmp_path, monkeypatch):
     items = mixed_batch()
     bcfg, order, ms, cached = autotune.tune_batch([s for s, _ in items], [o for _, o in items], reps=1)
     assert not cached and len(ms) == len(autotune.BATCH_CANDIDATES) and order in (0, 1, autotune.PLAIN)
+    got = zt.render_batch([s for s, _ in items], [o for _, o in items], bcfg)
+    for (s, o), img in zip(items, got):
+        assert img.pixels.tobytes() == zt.render(s, o).pixels.tobytes()
     assert autotune.tune_batch([s for s, _ in items], [o for _, o in items], reps=1)[3]  # cached now
 
 
@@ -80,6 +84,8 @@ def test_batch_rejects_bad_arguments():
     assert ei.value.name == "InvalidOptions"
     with pytest.raises(zt.ZigtraceError):
         zt.render_batch([s], [zt.Options(8, 8, 1, 4)], zt.GpuConfig(block_size=96))
+    with pytest.raises(zt.ZigtraceError):
+        zt.render_batch([s], [zt.Options(8, 8, 1, 4)], zt.GpuConfig(mode=zt.MODE_WAVEFRONT))
 
 
 def test_batch_without_lights_matches_oracle():

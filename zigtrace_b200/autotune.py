@@ -5,8 +5,9 @@ megakernel with path regeneration at 128/256, the wavefront form at three
 queue capacities (paths in flight: the default of one slot per pixel up to
 4M, 1M and 256K) and the sorted wavefront form at two.  For a batch it times the batched persistent launch
 at block sizes 64/128/256 with the renders in the given order or largest
-first, and the same renders as plain per-render launches (each with its own
-default choice) as one more candidate.  Every candidate renders identical
+first, its path-regeneration form at block sizes 128/256, and the same
+renders as plain per-render launches (each with its own default choice) as
+one more candidate.  Every candidate renders identical
 pixels at the caller's precision (the choice only changes scheduling), so
 the fastest one is kept; the precision itself is the caller's choice and is
 part of the cache key, since the exact and fast builds differ in their best
@@ -31,7 +32,9 @@ SINGLE_CANDIDATES: List[Tuple[int, int, int]] = [  # (mode, block_size, queue_ca
     (MODE_WAVEFRONT, 128, 0), (MODE_WAVEFRONT, 128, 1 << 20), (MODE_WAVEFRONT, 128, 1 << 18),
     (MODE_WAVEFRONT_SORTED, 128, 0), (MODE_WAVEFRONT_SORTED, 128, 1 << 20)]
 PLAIN = -1  # batch candidate: plain per-render launches instead of the batched launch
-BATCH_CANDIDATES: List[Tuple[int, int]] = [(bs, order) for bs in (64, 128, 256) for order in (0, 1)] + [(PLAIN, 0)]
+BATCH_CANDIDATES: List[Tuple[int, int, int]] = (  # (block_size, order, mode)
+    [(bs, order, MODE_MEGAKERNEL) for bs in (64, 128, 256) for order in (0, 1)] +
+    [(128, 1, MODE_MEGAKERNEL_REGEN), (256, 1, MODE_MEGAKERNEL_REGEN)] + [(PLAIN, 0, MODE_MEGAKERNEL)])
 
 
 def cache_path() -> Path:
@@ -154,7 +157,7 @@ def tune_batch(scenes: Sequence[Scene], opts: Sequence[Options], reps: int = 2,
             return
         if c not in batches:
             batches[c] = Batch(scenes, opts, [t.data_ptr() for t in outs],
-                               GpuConfig(block_size=c[0], precision=precision), order=c[1])
+                               GpuConfig(mode=c[2], block_size=c[0], precision=precision), order=c[1])
         batches[c].launch(stream)
 
     best, ms, cached = choose(f"{gpu_key()}|{batch_class(scenes, opts, precision)}", BATCH_CANDIDATES, run, reps,
@@ -164,4 +167,4 @@ def tune_batch(scenes: Sequence[Scene], opts: Sequence[Options], reps: int = 2,
         b.close()
     if best[0] == PLAIN:
         return GpuConfig(precision=precision), PLAIN, ms, cached
-    return GpuConfig(block_size=best[0], precision=precision), best[1], ms, cached
+    return GpuConfig(mode=best[2], block_size=best[0], precision=precision), best[1], ms, cached

@@ -502,6 +502,34 @@ __global__ void __launch_bounds__(BS, mega_threads_per_sm(kNee, kFast) / BS)
   }
 }
 
+/* The batched launch with per-lane path regeneration (render_pixel_regen):
+ * the same tiles and items, but a lane whose path ends starts its pixel's
+ * next sample at once.  Built like k_render_regen (four blocks of 128 per
+ * SM, 128 registers).  Every lane of a warp calls render_pixel_regen, lanes
+ * outside their image with valid = false. */
+template <int BS, bool kFast>
+__global__ void __launch_bounds__(BS, 512 / BS)
+    k_render_batch_regen(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t total_tiles,
+                         unsigned int* __restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if ((uint64_t)tile >= total_tiles) return;
+    uint32_t lo = 0, hi = n_items - 1; /* last item with tile_begin <= tile */
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) / 2;
+      if (items[mid].tile_begin <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchItem& it = items[lo];
+    const uint64_t local = tile - it.tile_begin;
+    const uint64_t x = (local % it.tiles_x) * 8 + (lane & 7), y = (local / it.tiles_x) * 4 + (lane >> 3);
+    render_pixel_regen<kFast>(it.sc, it.p, x, y, x < it.p.width && y < it.p.height, it.out);
+  }
+}
+
 __global__ void k_render_debug(DevScene sc, RenderParams p, int32_t* __restrict__ first_prim,
                                uint32_t* __restrict__ path_len) {
   const uint64_t pix = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1677,6 +1705,7 @@ struct zt_batch {
   uint32_t block_size = 128;
   bool nee = true; /* some render of the batch samples lights */
   bool fast = false; /* every render takes the fast traversal */
+  bool regen = false; /* the path-regeneration form of the batched kernel */
   BatchItem* d_items = nullptr;
   unsigned int* d_counter = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1691,8 +1720,20 @@ static void launch_batch_kernel(const zt_batch* b, cudaStream_t st) {
           b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
 }
 
+template <int BS, bool kFast>
+static void launch_batch_regen(const zt_batch* b, cudaStream_t st) {
+  k_render_batch_regen<BS, kFast>
+      <<<persistent_grid(k_render_batch_regen<BS, kFast>, BS, b->total_tiles * 32), BS, 0, st>>>(
+          b->d_items, (uint32_t)b->n, b->total_tiles, b->d_counter);
+}
+
 template <int BS>
 static void launch_batch_bs(const zt_batch* b, cudaStream_t st) {
+  if (b->regen) {
+    if (b->fast) launch_batch_regen<BS, true>(b, st);
+    else launch_batch_regen<BS, false>(b, st);
+    return;
+  }
   if (b->fast) {
     if (b->nee) launch_batch_kernel<BS, true, true>(b, st);
     else launch_batch_kernel<BS, false, true>(b, st);
@@ -1722,6 +1763,10 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
   const uint32_t bs = cfg ? cfg->block_size : 0;
   if (!valid_block_size(bs)) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_gpu_config.block_size must be 0, 64, 128 or 256");
   if (order > 1) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: order must be 0 (as given) or 1 (largest first)");
+  const uint32_t bmode = cfg ? cfg->mode : ZT_MODE_AUTO;
+  if (bmode != ZT_MODE_AUTO && bmode != ZT_MODE_MEGAKERNEL && bmode != ZT_MODE_MEGAKERNEL_REGEN)
+    return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: a batch runs the megakernel (mode 0 or 1) or its "
+                                         "path-regeneration form (mode 3)");
   std::vector<uint64_t> idx(n);
   std::vector<double> cost(n);
   for (uint64_t i = 0; i < n; ++i) {
@@ -1765,6 +1810,7 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
     return fail(ZT_ERR_INVALID_ARGUMENT, "unknown zt_gpu_config.precision");
   }
   b->fast = precision == ZT_PRECISION_FAST;
+  b->regen = bmode == ZT_MODE_MEGAKERNEL_REGEN;
   for (uint64_t k = 0; k < n && b->fast; ++k) b->fast = use_fast(scenes[idx[k]], items[k].p, precision);
   cudaError_t e = cudaGetDevice(&b->device);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_items, n * sizeof(BatchItem));

@@ -47,19 +47,39 @@ NCU_EXECUTION = {"triangle_heavy": {"issue_active_pct": 62.7, "lanes_per_warp_in
 NCU_DRAM_BYTES_BATCH = 0.160607e9 + 1.138117e9
 
 
+FP32_LANES_PER_SM = 128
+
+
 def roofline_entry(work: dict, samples: int, kernel_ms: float, sms: int, traffic, traffic_note: str,
                    execution) -> dict:
     """The roofline object for one kernel: oracle-counted FLOP and bytes per
-    sample times the samples of one launch, over its CUDA-event duration."""
+    sample times the samples of one launch, over its CUDA-event duration.
+    When part of the arithmetic is single precision (the fast traversal's box
+    tests, work["flop_f32"]), each part is set against its own pipe's peak and
+    frac is the share of the kernel's time that the arithmetic would take at
+    those peaks (f64 time + f32 time over kernel time)."""
     flop = work["flop"] * samples
+    f32 = work.get("flop_f32", 0.0) * samples
     achieved = flop / (kernel_ms / 1e3) / 1e12
     peak = sms * FP64_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+    peak32 = sms * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+    busy = ((flop - f32) / (peak * 1e12) + f32 / (peak32 * 1e12)) / (kernel_ms / 1e3)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     bytes_per_launch = work["bytes"] * samples
+    mixed = {}
+    if f32 > 0:
+        mixed = {"bound": "fp64+fp32",
+                 "split": {"fp64_tflops": round((flop - f32) / (kernel_ms / 1e3) / 1e12, 3),
+                           "fp64_peak": round(peak, 1),
+                           "fp32_tflops": round(f32 / (kernel_ms / 1e3) / 1e12, 3), "fp32_peak": round(peak32, 1),
+                           "note": "box tests in f32 (FMA) against the nominal FP32 peak, primitives and shading "
+                                   "in f64 against the nominal FP64 peak; frac = time the arithmetic needs at "
+                                   "those peaks over the kernel's time"}}
     return {
         "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
-        "frac": round(achieved / peak, 4),
+        "frac": round(busy, 4),
+        **mixed,
         "traffic": traffic, "traffic_note": traffic_note, "ncu_execution": execution,
         "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "
                        "no measured FP64 figure exists (the path uses no FMA: its issue-rate ceiling is half)",
@@ -69,7 +89,7 @@ def roofline_entry(work: dict, samples: int, kernel_ms: float, sms: int, traffic
         "memory": {"achieved_gbs": round(bytes_per_launch / (kernel_ms / 1e3) / 1e9, 1), "peak_gbs": hbm,
                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
                    "note": "bytes requested from the memory system; most are served by L2"},
-        "per_sample": {k: round(v, 3) for k, v in work.items() if k not in ("flop", "bytes")},
+        "per_sample": {k: round(v, 3) for k, v in work.items() if k not in ("flop", "bytes", "flop_f32")},
     }
 
 
@@ -425,7 +445,7 @@ def b200_arm(args):
         cpu = {"value": round(n_pix * o.spp / dt / 1e6, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",
                "sample": f"{n_pix} random pixels x {o.spp} spp ({n_pix * o.spp} samples), oracle C restatement "
                          f"of the reference CPU renderer, {threads} threads, {dt:.1f} s"}
-        work = workmodel.per_sample(st, o.spp, counts["nodes"] > 0)
+        work = workmodel.per_sample(st, o.spp, counts["nodes"] > 0, fast=prec == zt.PRECISION_FAST)
         queue_bytes = workmodel.wavefront_queue_bytes(st, o.spp)
         image_error = measured_image_error(scene, o, img, threads)
 
@@ -672,7 +692,7 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
             t_s += time.perf_counter() - t0
             n_s += len(pix) * o.spp
             w = o.width * o.height * o.spp
-            for key, v in workmodel.per_sample(st, o.spp).items():
+            for key, v in workmodel.per_sample(st, o.spp, fast=prec == zt.PRECISION_FAST).items():
                 work_w[key] = work_w.get(key, 0.0) + v * w
             weight += w
         cpu = {"value": round(n_s / t_s / 1e6, 4), "unit": "Msamples/s", "cores": threads, "kind": "port",

@@ -75,6 +75,20 @@ def test_roofline_entry_arithmetic():
     assert r["per_sample"] == {"ext_rays": 2.0, "shadow_rays": 0.5, "box_tests": 40.0, "prim_tests": 3.0}
 
 
+def test_roofline_with_single_precision_box_tests():
+    """Fast traversal: box-test FLOP against the FP32 peak, the rest against
+    FP64; frac is the time both need at peak over the kernel time."""
+    work = {"flop": 600.0, "flop_f32": 480.0, "bytes": 2000.0, "box_tests": 40.0}
+    r = bench.roofline_entry(work, samples=10_000_000, kernel_ms=5.0, sms=148, traffic=None, traffic_note="n",
+                             execution=None)
+    p64 = 148 * 64 * 2 * bench.NOMINAL_SM_MHZ * 1e6
+    p32 = 148 * 128 * 2 * bench.NOMINAL_SM_MHZ * 1e6
+    want = (120.0 * 1e7 / p64 + 480.0 * 1e7 / p32) / 5e-3
+    assert r["bound"] == "fp64+fp32" and r["frac"] == pytest.approx(want, abs=1e-4)  # frac has 4 decimals
+    assert r["split"]["fp32_tflops"] == pytest.approx(480.0 * 1e7 / 5e-3 / 1e12, rel=1e-3)
+    assert "flop_f32" not in r["per_sample"]
+
+
 def test_work_model_from_oracle_counters():
     scene = scenes.cornell().build()
     os_ = O.OracleScene.from_scene(scene)
@@ -88,6 +102,9 @@ def test_work_model_from_oracle_counters():
               workmodel.FLOP_SHADE * st["hits"] + workmodel.FLOP_NEE * st["nee_samples"]) / st["samples"]
     assert w["flop"] == pytest.approx(expect)
     assert w["bytes"] > workmodel.BYTES_PIXEL / 4
+    f = workmodel.per_sample(st, 4, fast=True)
+    assert f["flop"] == w["flop"] and f["flop_f32"] == pytest.approx(workmodel.FLOP_SLAB * st["slab_tests"] / st["samples"])
+    assert w["flop_f32"] == 0 and f["bytes"] < w["bytes"]
 
 
 def test_wavefront_queue_bytes():

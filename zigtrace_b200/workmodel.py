@@ -32,8 +32,14 @@ BYTES_PRIM = 80
 BYTES_PIXEL = 24
 
 
-def per_sample(stats: dict, spp: int, has_bvh: bool = True) -> dict:
-    """Per-sample FLOP and bytes from oracle counters (oracle.STATS_FIELDS)."""
+BYTES_FPAIR = 64  # the fast traversal's single-precision pair record
+
+
+def per_sample(stats: dict, spp: int, has_bvh: bool = True, fast: bool = False) -> dict:
+    """Per-sample FLOP and bytes from oracle counters (oracle.STATS_FIELDS).
+    With fast=True (the fast traversal) the box tests are single-precision
+    FMAs on 64-byte records: their FLOP are reported apart as flop_f32 and
+    the node records count 64 bytes."""
     n = max(stats["samples"], 1)
     traversals = (stats["ext_rays"] + stats["shadow_rays"]) if has_bvh else 0
     inner_pops = max(stats["slab_tests"] - traversals, 0) / 2
@@ -41,9 +47,11 @@ def per_sample(stats: dict, spp: int, has_bvh: bool = True) -> dict:
     flop = (FLOP_SLAB * stats["slab_tests"] + FLOP_SPHERE * stats["sphere_tests"] +
             FLOP_TRIANGLE * stats["tri_tests"] + FLOP_PLANE * stats["plane_tests"] + FLOP_SHADE * stats["hits"] +
             FLOP_NEE * stats["nee_samples"]) / n
-    nbytes = (BYTES_PAIR * inner_pops + BYTES_PRIM * prim_tests) / n + BYTES_PIXEL / spp
+    nbytes = ((BYTES_FPAIR if fast else BYTES_PAIR) * inner_pops + BYTES_PRIM * prim_tests) / n + BYTES_PIXEL / spp
+    flop_f32 = FLOP_SLAB * stats["slab_tests"] / n if fast else 0.0
     return {
         "flop": flop,
+        "flop_f32": flop_f32,
         "bytes": nbytes,
         "ext_rays": stats["ext_rays"] / n,
         "shadow_rays": stats["shadow_rays"] / n,

@@ -35,16 +35,20 @@ NOMINAL_SM_MHZ = 1965.0
 # DRAM bytes (read + write) per sample of the megakernel, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, one 8-spp launch of the
 # workload, --clock-control none) and scaled by samples per launch: traffic
-# grows with the samples traced.  Workloads without a capture report null.
-NCU_DRAM_BYTES_PER_SAMPLE = {"triangle_heavy": 2.527835e9 / (1920 * 1080 * 8)}
+# grows with the samples traced.  Keyed by (workload, precision); workloads
+# without a capture report null.
+NCU_DRAM_BYTES_PER_SAMPLE = {("triangle_heavy", "exact"): 2.527835e9 / (1920 * 1080 * 8)}
 # What bounds the kernel instead of a pipe peak, from the same capture:
 # issue slots used, lanes active per warp instruction, FP64 pipe activity.
-NCU_EXECUTION = {"triangle_heavy": {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
-                                    "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
-                 "batch": {"issue_active_pct": 70.2, "lanes_per_warp_instruction": 14.23,
-                           "fp64_pipe_active_pct": 44.5, "l1_hit_pct": 82.9, "l2_hit_pct": 88.5}}
-# The batched launch, captured whole (rank 0's batch, one launch).
-NCU_DRAM_BYTES_BATCH = 0.160607e9 + 1.138117e9
+NCU_EXECUTION = {("triangle_heavy", "exact"): {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
+                                               "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
+                 ("batch", "exact"): {"issue_active_pct": 70.2, "lanes_per_warp_instruction": 14.23,
+                                      "fp64_pipe_active_pct": 44.5, "l1_hit_pct": 82.9, "l2_hit_pct": 88.5},
+                 ("batch", "fast"): {"issue_active_pct": 59.5, "lanes_per_warp_instruction": 14.33,
+                                     "fp64_pipe_active_pct": 19.9, "l1_hit_pct": 80.4, "l2_hit_pct": 88.4,
+                                     "top_stall": "no_instruction 3.5 cycles per issue"}}
+# The batched launch, captured whole (rank 0's batch, one launch), by precision.
+NCU_DRAM_BYTES_BATCH = {"exact": 0.160607e9 + 1.138117e9, "fast": 0.100172e9 + 1.266429e9}
 
 
 FP32_LANES_PER_SM = 128
@@ -454,10 +458,10 @@ def b200_arm(args):
         sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
         roofline = roofline_entry(
             work, samples, kernel_ms, sms,
-            (round(NCU_DRAM_BYTES_PER_SAMPLE[args.workload] * samples)
-             if args.workload in NCU_DRAM_BYTES_PER_SAMPLE and gcfg.mode in (0, 1) else None),
+            (round(NCU_DRAM_BYTES_PER_SAMPLE[(args.workload, args.precision)] * samples)
+             if (args.workload, args.precision) in NCU_DRAM_BYTES_PER_SAMPLE and gcfg.mode in (0, 1) else None),
             "DRAM bytes per launch from an ncu capture of an 8-spp launch, scaled by samples",
-            NCU_EXECUTION.get(args.workload) if gcfg.mode in (0, 1) else None)
+            NCU_EXECUTION.get((args.workload, args.precision)) if gcfg.mode in (0, 1) else None)
         if gcfg.mode in (2, 4):  # the wavefront form: path-state traffic through HBM against the copy peak
             qbps = queue_bytes * samples / (kernel_ms / 1e3) / 1e9
             roofline["queue"] = {"bytes_per_sample": round(queue_bytes, 1), "achieved_gbs": round(qbps, 1),
@@ -699,9 +703,10 @@ def batch_arm(args, world, rank, local_rank, barrier, allmax):
                "sample": f"1024 random pixels x 16 spp from each of 32 random renders of the batch ({n_s} samples)"}
         sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
         roofline = roofline_entry(
-            {key: v / weight for key, v in work_w.items()}, samples, batch_ms, sms, round(NCU_DRAM_BYTES_BATCH),
+            {key: v / weight for key, v in work_w.items()}, samples, batch_ms, sms,
+            round(NCU_DRAM_BYTES_BATCH[args.precision]),
             "DRAM bytes of one batched launch of this batch (seed 0), from an ncu capture",
-            NCU_EXECUTION["batch"])
+            NCU_EXECUTION.get(("batch", args.precision)))
         roofline["work_note"] = ("per-sample work averaged over 32 sampled renders, each weighted by its samples "
                                  "per step")
 

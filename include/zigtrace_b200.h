@@ -91,7 +91,9 @@ enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_
        ZT_MODE_WAVEFRONT_SORTED = 4 };
 /* ZT_PRECISION_EXACT (the default) is the verification build of the path:
  * every operation is the reference's f64 operation in the reference's order,
- * so images are bit-identical to the reference algorithm's.
+ * so images are bit-identical to the reference algorithm's as restated by
+ * the project's CPU oracle (which shares this library's sin/cos, so parity
+ * with Zig's own transcendentals is not covered).
  * ZT_PRECISION_FAST tests BVH boxes in single precision against conservative
  * (outward-rounded, widened) copies of the f64 boxes; primitive tests, hit
  * records and shading stay the reference's f64 operations.  It visits every

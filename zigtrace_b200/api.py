@@ -157,7 +157,7 @@ class Options:
 @dataclass
 class GpuConfig:
     """Device execution choices (zt_gpu_config); zeros mean defaults.
-    ``precision``: PRECISION_EXACT (bit-identical to the reference
+    ``precision``: PRECISION_EXACT (bit-identical to the CPU oracle's restatement of the reference
     algorithm) or PRECISION_FAST (single-precision conservative BVH boxes,
     f64 everything else)."""
     mode: int = MODE_AUTO

@@ -100,8 +100,11 @@ enum { ZT_MODE_AUTO = 0, ZT_MODE_MEGAKERNEL = 1, ZT_MODE_WAVEFRONT = 2, ZT_MODE_
  * BVH leaf the exact walk visits (and some more), so the closest hit differs
  * only on exact ties and rays that graze a box edge: images agree with the
  * exact ones to far below Monte Carlo noise, though not bit for bit.  Used by
- * the megakernel modes and the batch; scenes whose leaves hold more than 15
- * primitives or whose bounds or camera exceed 1e7 in magnitude render exact. */
+ * the megakernel modes and the batch; single renders of scenes with fewer
+ * than 64 bounded primitives (where the float walk does not pay), and any
+ * render whose scene has leaves of more than 15 primitives or bounds or a
+ * camera beyond 1e7 in magnitude, render exact (a batch takes the fast walk
+ * only if all of its renders can). */
 enum { ZT_PRECISION_EXACT = 0, ZT_PRECISION_FAST = 1 };
 typedef struct {
   uint32_t mode;           /* ZT_MODE_* */

@@ -8,7 +8,9 @@ fast walk reaches every BVH leaf the f64 walk reaches, so paths differ only
 where a closest hit is decided by a tie or a grazing box test: the tests
 also require nearly every pixel to be bit-identical to the oracle's.
 Renders the float records cannot serve (a camera beyond their coordinate
-range) fall back to the exact walk and must then be bit-identical.
+range) and single renders of scenes under 64 bounded primitives take the
+exact walk and must then be bit-identical; the scenes of the statistical
+tests carry an extra 320-triangle icosphere to stay above that size.
 """
 import numpy as np
 import pytest
@@ -23,6 +25,28 @@ pytestmark = pytest.mark.gpu
 
 FAST = zt.GpuConfig(precision=zt.PRECISION_FAST)
 MODES = [pytest.param(zt.MODE_MEGAKERNEL, id="mega"), pytest.param(zt.MODE_MEGAKERNEL_REGEN, id="regen")]
+FAST_MIN_PRIMITIVES = 64  # single renders of smaller scenes take the exact walk
+
+
+def _denser(scene, center, radius, material=0, seed=0):
+    """Adds a 320-triangle icosphere so that a single render of the scene
+    takes the fast walk (at least 64 bounded primitives)."""
+    verts, faces = scenes.icosphere(2)
+    v = np.asarray(verts) * radius + np.asarray(center, float)
+    f = np.asarray(faces)
+    scene.add_triangles(v[f[:, 0]], v[f[:, 1]], v[f[:, 2]], material)
+    assert scene.primitive_count() - 1 >= FAST_MIN_PRIMITIVES
+    return scene
+
+
+def cornell_dense():
+    s = scenes.cornell()
+    return _denser(s, (400, 330, 200), 60.0, material=2)
+
+
+def fuzz_dense(seed):
+    s = K.fuzz_scene(seed)
+    return _denser(s, (1.5, 0.6, -3.5), 0.5, material=0)
 
 
 def _whole(scene, o, cfg):
@@ -43,7 +67,7 @@ def _subset(scene, o, cfg, n, seed):
 
 @pytest.mark.parametrize("mode", MODES)
 def test_cornell_full_size(mode):
-    a = _whole(scenes.cornell().build(), scenes.CORNELL_OPTIONS, zt.GpuConfig(mode, precision=zt.PRECISION_FAST))
+    a = _whole(cornell_dense().build(), scenes.CORNELL_OPTIONS, zt.GpuConfig(mode, precision=zt.PRECISION_FAST))
     assert a["ok"], a
     assert a["identical_pixels"] > 0.99, a
 
@@ -65,14 +89,14 @@ def test_triangle_heavy_benchmark_config_subset():
 @pytest.mark.parametrize("seed", range(8))
 def test_fuzz_scenes(seed):
     """Every shape, material and light kind, lens sampling, both backgrounds."""
-    scene = K.fuzz_scene(seed).build()
+    scene = fuzz_dense(seed).build()
     a = _whole(scene, zt.Options(64, 48, 16, 12, seed=seed), FAST)
     assert a["ok"], a
     assert a["identical_pixels"] > 0.98, a
 
 
 def test_light_sampling_off_and_batch():
-    scene = scenes.cornell().build()
+    scene = cornell_dense().build()
     o = zt.Options(96, 96, 8, 16, light_sampling=False)
     a = _whole(scene, o, FAST)
     assert a["ok"], a
@@ -89,11 +113,20 @@ def test_camera_outside_the_float_range_renders_exact():
     """A camera farther than 1e7 from the origin is outside the range the
     float test handles: the render falls back to the f64 walk and is
     bit-identical to the oracle."""
-    far = scenes.cornell()
+    far = cornell_dense()
     far.camera = zt.CameraConfig(look_from=(278, 278, -2e7), look_at=(278, 278, 0), vfov=0.01)
     far.build()
     o = zt.Options(64, 64, 4, 8)
     assert zt.render(far, o, FAST).pixels.tobytes() == O.OracleScene.from_scene(far).render(64, 64, 4, 8).tobytes()
+
+
+def test_small_scene_single_render_is_exact():
+    """Below 64 bounded primitives a single render takes the exact walk: the
+    fast precision then gives the oracle's pixels bit for bit."""
+    scene = scenes.cornell().build()
+    o = zt.Options(64, 64, 4, 16)
+    want = O.OracleScene.from_scene(scene).render(64, 64, 4, 16)
+    assert zt.render(scene, o, FAST).pixels.tobytes() == want.tobytes()
 
 
 def test_fast_is_deterministic():

@@ -36,15 +36,16 @@ def test_imported_tree_renders_bit_exact(make, o, mode):
 
 
 def test_one_big_leaf_renders_exact_under_fast():
-    """A tree that is a single leaf of 40 triangles: more than the 15 a packed
-    fast record holds, so PRECISION_FAST renders with the f64 walk; a tree of
-    one leaf is also what Scene.intersect's brute-force loop tests
-    (scene.zig:109-112)."""
+    """A tree that is a single leaf of 80 primitives: more than the 15 a
+    packed fast record holds (and more than the 64 below which a single
+    render takes the exact walk anyway), so PRECISION_FAST renders with the
+    f64 walk; a tree of one leaf is also what Scene.intersect's brute-force
+    loop tests (scene.zig:109-112)."""
     scene = scenes.cornell()
     n = scene.primitive_count()
     rng = np.random.default_rng(3)
     m = scene.add_material(zt.Material.lambertian((0.3, 0.6, 0.2)))
-    c = rng.uniform(100, 450, (40 - n, 3))
+    c = rng.uniform(100, 450, (80 - n, 3))
     scene.add_triangles(c, c + rng.uniform(-40, 40, c.shape), c + rng.uniform(-40, 40, c.shape), m)
     n = scene.primitive_count()
     shapes = scene.shapes

@@ -326,13 +326,16 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
 constexpr int kMegaThreadsPerSm = 896;
 constexpr int kMegaThreadsPerSmNoNee = 896;
 #ifndef ZT_FAST_THREADS_PER_SM
-#define ZT_FAST_THREADS_PER_SM 896
+#define ZT_FAST_THREADS_PER_SM 1024
 #endif
 #ifndef ZT_FAST_THREADS_PER_SM_NONEE
-#define ZT_FAST_THREADS_PER_SM_NONEE 896
+#define ZT_FAST_THREADS_PER_SM_NONEE 1024
 #endif
 /* Resident threads per SM each megakernel and batch instance is built for
- * (__launch_bounds__): sets the register budget, 65,536 / threads. */
+ * (__launch_bounds__): sets the register budget, 65,536 / threads.  The
+ * fast-walk instances measured fastest at 1024 (64 registers): on the
+ * 1M-triangle terrain 1026 Msamples/s against 992 at 896 and 933 at 768; on
+ * the sphere-field batch 64.4 ms against 67.9 at 896 and 71.7 at 1280. */
 __host__ __device__ constexpr int mega_threads_per_sm(bool nee, bool fast) {
   return fast ? (nee ? ZT_FAST_THREADS_PER_SM : ZT_FAST_THREADS_PER_SM_NONEE)
               : (nee ? kMegaThreadsPerSm : kMegaThreadsPerSmNoNee);
@@ -897,12 +900,18 @@ static void launch_mega_bs(const DevScene& v, const RenderParams& p, double* d_o
 
 static bool valid_block_size(uint32_t bs) { return bs == 0 || bs == 64 || bs == 128 || bs == 256; }
 
-/* Whether a render takes the fast traversal: asked for, and the scene has
- * its float records (a scene whose leaves or bounds do not fit them renders
- * with the f64 traversal).  The camera origin must be within the records'
- * coordinate range as well. */
-static bool use_fast(const zt_scene* s, const RenderParams& p, uint32_t precision) {
+/* Whether a render takes the fast traversal: asked for, the scene has its
+ * float records (a scene whose leaves or bounds do not fit them renders
+ * with the f64 traversal) and, for a single render, at least
+ * kFastMinPrimitives bounded primitives.  The camera origin must be within
+ * the records' coordinate range as well. */
+constexpr uint32_t kFastMinPrimitives = 64;
+static bool use_fast(const zt_scene* s, const RenderParams& p, uint32_t precision, bool small_scenes_exact = true) {
   if (precision != ZT_PRECISION_FAST || !s->device || !s->device->view.fast_ok) return false;
+  /* on a tree this small the float walk's per-ray set-up costs more than its
+   * box tests save (Cornell box, 14 primitives: 477 vs 565 Msamples/s); a
+   * batch, whose renders share one kernel instance, skips this rule */
+  if (small_scenes_exact && s->device->view.n_prims < kFastMinPrimitives) return false;
   const double* o = p.cam.origin;
   const double reach = fabs(p.cam.lens_radius) * (fabs(p.cam.u[0]) + fabs(p.cam.u[1]) + fabs(p.cam.u[2]) +
                                                   fabs(p.cam.v[0]) + fabs(p.cam.v[1]) + fabs(p.cam.v[2]));
@@ -1811,7 +1820,7 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
   }
   b->fast = precision == ZT_PRECISION_FAST;
   b->regen = bmode == ZT_MODE_MEGAKERNEL_REGEN;
-  for (uint64_t k = 0; k < n && b->fast; ++k) b->fast = use_fast(scenes[idx[k]], items[k].p, precision);
+  for (uint64_t k = 0; k < n && b->fast; ++k) b->fast = use_fast(scenes[idx[k]], items[k].p, precision, false);
   cudaError_t e = cudaGetDevice(&b->device);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_items, n * sizeof(BatchItem));
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_counter, sizeof(unsigned int));

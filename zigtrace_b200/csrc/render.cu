@@ -218,7 +218,11 @@ static zt_status make_staging(zt_scene* s) {
 
 static zt_status pilot_paths(zt_scene* s);
 
-static zt_status upload(zt_scene* s) {
+/* Makes the scene resident on the current device.  With sync = false the
+ * host-to-device copy is left in flight on the legacy default stream (work
+ * later enqueued there, or after a synchronisation, sees it): a caller
+ * uploading many scenes synchronises once. */
+static zt_status upload(zt_scene* s, bool sync = true) {
   if (!s->built) return fail(ZT_ERR_NOT_BUILT, "scene is not built: call zt_scene_build first");
   int dev = 0;
   ZT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
@@ -238,7 +242,7 @@ static zt_status upload(zt_scene* s) {
     return arc;
   }
   cudaError_t e = cudaMemcpyAsync(d->block, h->pinned, h->bytes, cudaMemcpyHostToDevice, 0);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  if (e == cudaSuccess && sync) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     release_device(s);
     return cuda_fail(e, "upload scene");
@@ -1782,13 +1786,14 @@ zt_status zt_batch_create(zt_scene* const* scenes, const zt_options* opts, uint6
     zt_status rc = check_render_args(scenes[i], &opts[i]);
     if (rc != ZT_OK) return rc;
     if (!d_outs[i]) return fail(ZT_ERR_INVALID_ARGUMENT, "zt_batch_create: NULL output");
-    rc = upload(scenes[i]);
+    rc = upload(scenes[i], false); /* copies in flight; one synchronisation below */
     if (rc != ZT_OK) return rc;
     idx[i] = i;
     /* expected work: samples x log2 of the primitive count */
     cost[i] = (double)(opts[i].width * opts[i].height * opts[i].spp) *
               log2((double)scenes[i]->shapes.size() + scenes[i]->planes.size() + 2.0);
   }
+  ZT_CUDA(cudaStreamSynchronize(0), "upload the batch's scenes");
   if (order == 1) std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return cost[a] > cost[b]; });
   std::vector<BatchItem> items(n);
   uint64_t tiles = 0;
@@ -1865,21 +1870,22 @@ zt_status zt_render_batch(zt_scene* const* scenes, const zt_options* opts, uint6
     off[i + 1] = off[i] + (size_t)(opts[i].width * opts[i].height * 3);
   }
   double* d = nullptr;
-  ZT_CUDA(cudaMalloc((void**)&d, off[n] * sizeof(double)), "allocate batch framebuffers");
+  zt_status rc = pool_alloc((void**)&d, off[n] * sizeof(double), 0, "allocate batch framebuffers");
+  if (rc != ZT_OK) return rc;
   std::vector<double*> d_outs(n);
   for (uint64_t i = 0; i < n; ++i) d_outs[i] = d + off[i];
   zt_batch* b = nullptr;
-  zt_status rc = zt_batch_create(scenes, opts, n, d_outs.data(), cfg, 1, &b);
+  rc = zt_batch_create(scenes, opts, n, d_outs.data(), cfg, 1, &b);
   if (rc == ZT_OK) rc = zt_batch_launch(b, nullptr);
-  if (rc == ZT_OK) {
-    for (uint64_t i = 0; i < n && rc == ZT_OK; ++i) {
-      const cudaError_t e = cudaMemcpy(outs[i], d_outs[i], (off[i + 1] - off[i]) * sizeof(double),
-                                       cudaMemcpyDeviceToHost);
-      if (e != cudaSuccess) rc = cuda_fail(e, "copy batch framebuffer");
-    }
+  if (rc == ZT_OK) { /* every image back, then one synchronisation */
+    cudaError_t e = cudaSuccess;
+    for (uint64_t i = 0; i < n && e == cudaSuccess; ++i)
+      e = cudaMemcpyAsync(outs[i], d_outs[i], (off[i + 1] - off[i]) * sizeof(double), cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) rc = cuda_fail(e, "copy batch framebuffers");
   }
   zt_batch_destroy(b);
-  cudaFree(d);
+  pool_free(d, 0);
   return rc;
 }
 

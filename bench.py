@@ -37,11 +37,15 @@ NOMINAL_SM_MHZ = 1965.0
 # workload, --clock-control none) and scaled by samples per launch: traffic
 # grows with the samples traced.  Keyed by (workload, precision); workloads
 # without a capture report null.
-NCU_DRAM_BYTES_PER_SAMPLE = {("triangle_heavy", "exact"): 2.527835e9 / (1920 * 1080 * 8)}
+NCU_DRAM_BYTES_PER_SAMPLE = {("triangle_heavy", "exact"): 2.527835e9 / (1920 * 1080 * 8),
+                             ("triangle_heavy", "fast"): (1.138160e9 + 1.444120e9) / (1920 * 1080 * 8)}
 # What bounds the kernel instead of a pipe peak, from the same capture:
 # issue slots used, lanes active per warp instruction, FP64 pipe activity.
 NCU_EXECUTION = {("triangle_heavy", "exact"): {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
                                                "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
+                 ("triangle_heavy", "fast"): {"issue_active_pct": 62.5, "lanes_per_warp_instruction": 7.38,
+                                              "fp64_pipe_active_pct": 31.6, "fma_pipe_active_pct": 9.2,
+                                              "l1_hit_pct": 76.2, "l2_hit_pct": 83.7},
                  ("batch", "exact"): {"issue_active_pct": 70.2, "lanes_per_warp_instruction": 14.23,
                                       "fp64_pipe_active_pct": 44.5, "l1_hit_pct": 82.9, "l2_hit_pct": 88.5},
                  ("batch", "fast"): {"issue_active_pct": 59.5, "lanes_per_warp_instruction": 14.33,

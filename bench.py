@@ -494,9 +494,9 @@ def b200_arm(args):
         sub.steps, sub.warmup, sub.spp = min(args.steps, 10), 3, 0
         del out, flush
         torch.cuda.empty_cache()
-        line["batch"] = batch_arm(sub, world, rank, local_rank, barrier, allmax)
+        line["diff"] = diff_arm(sub, world, rank, local_rank, barrier, allmax)  # host-timed: before the batch's load
         torch.cuda.empty_cache()
-        line["diff"] = diff_arm(sub, world, rank, local_rank, barrier, allmax)
+        line["batch"] = batch_arm(sub, world, rank, local_rank, barrier, allmax)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -35,8 +35,8 @@ using namespace zt;
 struct zt_host_staging {
   void* pinned = nullptr;
   size_t bytes = 0;
-  size_t off_prims = 0, off_ids = 0, off_pairs = 0, off_fpairs = 0, off_wnodes = 0, off_planes = 0, off_mats = 0,
-         off_lights = 0, off_cdf = 0;
+  size_t off_prims = 0, off_ids = 0, off_pairs = 0, off_fpairs = 0, off_planes = 0, off_mats = 0, off_lights = 0,
+         off_cdf = 0;
   DevScene view;  /* counts, root, total; pointers unset */
 };
 
@@ -192,7 +192,6 @@ static zt_status make_staging(zt_scene* s) {
   stage(f.prim_ids, cur, h->off_ids);
   stage(f.pairs, cur, h->off_pairs);
   stage(f.fpairs, cur, h->off_fpairs);
-  stage(f.wnodes, cur, h->off_wnodes);
   stage(f.planes, cur, h->off_planes);
   stage(f.mats, cur, h->off_mats);
   stage(f.lights, cur, h->off_lights);
@@ -208,7 +207,6 @@ static zt_status make_staging(zt_scene* s) {
   stage_copy(f.prim_ids, h->pinned, h->off_ids);
   stage_copy(f.pairs, h->pinned, h->off_pairs);
   stage_copy(f.fpairs, h->pinned, h->off_fpairs);
-  stage_copy(f.wnodes, h->pinned, h->off_wnodes);
   stage_copy(f.planes, h->pinned, h->off_planes);
   stage_copy(f.mats, h->pinned, h->off_mats);
   stage_copy(f.lights, h->pinned, h->off_lights);
@@ -255,7 +253,6 @@ static zt_status upload(zt_scene* s, bool sync = true) {
   d->view.prim_ids = (const int32_t*)(b + h->off_ids);
   d->view.pairs = (const DPair*)(b + h->off_pairs);
   d->view.fpairs = h->view.fast_ok ? (const FPair*)(b + h->off_fpairs) : nullptr;
-  d->view.wnodes = h->view.fast_ok ? (const WNode*)(b + h->off_wnodes) : nullptr;
   d->view.planes = (const DPrim*)(b + h->off_planes);
   d->view.mats = (const DMat*)(b + h->off_mats);
   d->view.lights = (const DLight*)(b + h->off_lights);

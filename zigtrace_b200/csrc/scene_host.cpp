@@ -446,75 +446,6 @@ static float f32_up(double x) {
   return f;
 }
 
-/* The 4-wide tree of the fast walk (zt_types.h WNode), collapsed from the
- * binary tree: a wide node starts as a binary node's two children and
- * repeatedly replaces its interior child of largest surface area by that
- * child's two children until it holds four (or only leaves).  Every binary
- * leaf ends up under exactly one wide node, with the same primitives, and a
- * wide node is never deeper than the binary nodes it holds.  Boxes are the
- * binary nodes' boxes moved outward by eps and rounded outward, as in the
- * binary float records. */
-static void make_wide_tree(const zt_scene* s, const double eps[3], FlatScene* f) {
-  DevScene& v = f->view;
-  f->wnodes.clear();
-  const std::vector<HostNode>& nd = s->nodes;
-  auto leaf_word = [&](uint32_t c) { return (nd[c].count << kFastCountShift) | nd[c].first; };
-  if (nd[0].count > 0) {
-    v.wroot_word = leaf_word(0);
-    return;
-  }
-  auto area = [&](uint32_t c) {
-    const double dx = nd[c].bmax[0] - nd[c].bmin[0], dy = nd[c].bmax[1] - nd[c].bmin[1],
-                 dz = nd[c].bmax[2] - nd[c].bmin[2];
-    return dx * dy + dy * dz + dz * dx;
-  };
-  f->wnodes.reserve(nd.size() / 2 + 1);
-  /* explicit stack of (binary interior node, wide slot to fill) */
-  std::vector<std::pair<uint32_t, uint32_t>> todo;
-  f->wnodes.push_back(WNode{});
-  todo.emplace_back(0u, 0u);
-  while (!todo.empty()) {
-    const uint32_t b = todo.back().first, wi = todo.back().second;
-    todo.pop_back();
-    uint32_t ch[4] = {nd[b].first, nd[b].first + 1, 0, 0};
-    int nc = 2;
-    while (nc < 4) {
-      int best = -1;
-      double best_area = -1.0;
-      for (int i = 0; i < nc; ++i)
-        if (nd[ch[i]].count == 0 && area(ch[i]) > best_area) {
-          best = i;
-          best_area = area(ch[i]);
-        }
-      if (best < 0) break;
-      const uint32_t c = ch[best];
-      ch[best] = nd[c].first;
-      ch[nc++] = nd[c].first + 1;
-    }
-    WNode w{};
-    for (int i = 0; i < 4; ++i) {
-      if (i >= nc) {
-        w.word[i] = kWideEmpty;
-        continue;
-      }
-      const HostNode& c = nd[ch[i]];
-      for (int k = 0; k < 3; ++k) {
-        w.lo[k][i] = f32_down(c.bmin[k] - eps[k]);
-        w.hi[k][i] = f32_up(c.bmax[k] + eps[k]);
-      }
-      if (c.count > 0) {
-        w.word[i] = leaf_word(ch[i]);
-      } else {
-        w.word[i] = (uint32_t)f->wnodes.size();
-        f->wnodes.push_back(WNode{});
-        todo.emplace_back(ch[i], w.word[i]);
-      }
-    }
-    f->wnodes[wi] = w;
-  }
-  v.wroot_word = 0;
-}
-
 /* The fast traversal's float records (zt_types.h FPair): every box of the
  * f64 tree moved outward by eps[axis] = 2^-20 * M[axis], M the largest
  * |bound| of the root box on that axis, then rounded outward.  The margin
@@ -560,7 +491,6 @@ static void make_fast_records(const zt_scene* s, FlatScene* f) {
     v.froot_hi[k] = f32_up(s->nodes[0].bmax[k] + eps[k]);
   }
   v.froot_word = word(0);
-  make_wide_tree(s, eps, f);
   v.fast_ok = 1;
 }
 

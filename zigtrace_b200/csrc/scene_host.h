@@ -34,7 +34,6 @@ struct FlatScene {
   std::vector<int32_t> prim_ids;
   std::vector<DPair> pairs;
   std::vector<FPair> fpairs; /* conservative float copy of pairs (empty when the fast traversal cannot be used) */
-  std::vector<WNode> wnodes; /* the same boxes as a 4-wide tree (empty when fpairs is) */
   std::vector<DPrim> planes;
   std::vector<DMat> mats;
   std::vector<DLight> lights;

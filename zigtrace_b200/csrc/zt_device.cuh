@@ -413,12 +413,6 @@ ZT_D bool scene_occluded(const DevScene& sc, dv3 o, dv3 d, double tmin, double t
 
 #include "zt_fast.cuh"
 
-/* The fast walk's tree: 1 = the 4-wide tree (WNode), 0 = the binary float
- * records (FPair). */
-#ifndef ZT_FAST_WIDE
-#define ZT_FAST_WIDE 1
-#endif
-
 namespace zt {
 
 /* Closest or any hit with the hit record (kAnyHit: t only).  kFast walks
@@ -426,8 +420,7 @@ namespace zt {
 template <bool kAnyHit, bool kFast = false>
 ZT_D bool scene_intersect(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, Hit& out) {
   double t;
-  const int32_t k = (kFast && !kAnyHit) ? (ZT_FAST_WIDE ? scene_query_wide(sc, o, d, tmin, tmax, t)
-                                                        : scene_query_fast(sc, o, d, tmin, tmax, t))
+  const int32_t k = (kFast && !kAnyHit) ? scene_query_fast(sc, o, d, tmin, tmax, t)
                                         : scene_query<kAnyHit>(sc, o, d, tmin, tmax, t);
   if (k == -1) return false;
   out.t = t;
@@ -625,8 +618,7 @@ ZT_D dv3 direct_light(const DevScene& sc, dv3 albedo, const Hit& hit, Rng& rng) 
   const double cos_s = vdot(hit.normal, ldir);
   if (cos_s <= 0 || !(lpdf > 0)) return V(0, 0, 0);
   const double shadow_tmax = ldist * (1 - 1e-6);
-  if (kFast ? (ZT_FAST_WIDE ? scene_occluded_wide(sc, hit.point, ldir, kRayEpsilon, shadow_tmax)
-                            : scene_occluded_fast(sc, hit.point, ldir, kRayEpsilon, shadow_tmax))
+  if (kFast ? scene_occluded_fast(sc, hit.point, ldir, kRayEpsilon, shadow_tmax)
             : scene_occluded(sc, hit.point, ldir, kRayEpsilon, shadow_tmax))
     return V(0, 0, 0);
   const double bsdf_pdf = cos_s / kPi;

@@ -250,159 +250,6 @@ ZT_D bool scene_occluded_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
   return false;
 }
 
-/* ---------------------------------------------------- 4-wide tree walks */
-
-/* Compare-exchange of (key, word) pairs into ascending key order. */
-ZT_D void wcswap(float& ka, uint32_t& wa, float& kb, uint32_t& wb) {
-  const bool sw = kb < ka;
-  const float k = sw ? kb : ka;
-  const uint32_t w = sw ? wb : wa;
-  kb = sw ? ka : kb;
-  wb = sw ? wa : wb;
-  ka = k;
-  wa = w;
-}
-
-/* The four children of one wide node: entry distance (+inf when missed or
- * unused) and payload word. */
-ZT_D void wide_children(const WNode* node, const FRay& fr, float tmin, float tmax, float k[4], uint32_t w[4]) {
-  const float4* q = reinterpret_cast<const float4*>(node);
-  const float4 lx = __ldg(q), ly = __ldg(q + 1), lz = __ldg(q + 2);
-  const float4 hx = __ldg(q + 3), hy = __ldg(q + 4), hz = __ldg(q + 5);
-  const uint4 ww = __ldg(reinterpret_cast<const uint4*>(q + 6));
-  float t;
-  k[0] = (ww.x != kWideEmpty && fslab(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, fr, tmin, tmax, t)) ? t : INFINITY;
-  k[1] = (ww.y != kWideEmpty && fslab(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, fr, tmin, tmax, t)) ? t : INFINITY;
-  k[2] = (ww.z != kWideEmpty && fslab(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, fr, tmin, tmax, t)) ? t : INFINITY;
-  k[3] = (ww.w != kWideEmpty && fslab(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, fr, tmin, tmax, t)) ? t : INFINITY;
-  w[0] = ww.x;
-  w[1] = ww.y;
-  w[2] = ww.z;
-  w[3] = ww.w;
-}
-
-/* scene_query_fast over the 4-wide tree: the children a node's box test
- * reaches are visited nearest first (sorted by float entry distance), the
- * others pushed farthest first; pruning and primitive tests as in the
- * binary walk.  The leaves reached are the binary walk's (each wide node
- * holds binary nodes and tests their own boxes), so the superset property
- * and the closest hit carry over. */
-ZT_D int32_t scene_query_wide(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax, double& t_out) {
-  double closest = tmax;
-  int32_t best_k = -1;
-  if (sc.has_root) {
-    FRay fr;
-    if (!fray_make(o, d, fr)) return scene_query_exact_outlined(sc, o, d, tmin, tmax, t_out);
-    const float tmin32 = __double2float_rd(tmin);
-    float cl32 = __double2float_ru(closest);
-    float t;
-    if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
-              tmin32, cl32, t)) {
-      uint2 stack[kWideStackSize]; /* (payload word, entry distance bits) */
-      uint32_t w = sc.wroot_word;
-      float et = t;
-      bool have = true;
-      int sp = 0;
-      for (;;) {
-        if (!have) {
-          if (sp == 0) break;
-          const uint2 e = stack[--sp];
-          w = e.x;
-          et = __uint_as_float(e.y);
-        }
-        have = false;
-        if (et > cl32) continue; /* bvh.zig:97, against closest rounded up */
-        const uint32_t cnt = w >> kFastCountShift, first = w & kFastFirstMask;
-        if (cnt > 0) {
-          for (uint32_t k = first; k < first + cnt; ++k) {
-            double th;
-            if (prim_t(sc.prims[k], o, d, tmin, closest, th)) {
-              closest = th;
-              best_k = (int32_t)k;
-              cl32 = __double2float_ru(th);
-            }
-          }
-          continue;
-        }
-        float k[4];
-        uint32_t cw[4];
-        wide_children(sc.wnodes + first, fr, tmin32, cl32, k, cw);
-        wcswap(k[0], cw[0], k[1], cw[1]); /* sorting network for four */
-        wcswap(k[2], cw[2], k[3], cw[3]);
-        wcswap(k[0], cw[0], k[2], cw[2]);
-        wcswap(k[1], cw[1], k[3], cw[3]);
-        wcswap(k[1], cw[1], k[2], cw[2]);
-        if (k[3] < INFINITY) stack[sp++] = make_uint2(cw[3], __float_as_uint(k[3]));
-        if (k[2] < INFINITY) stack[sp++] = make_uint2(cw[2], __float_as_uint(k[2]));
-        if (k[1] < INFINITY) stack[sp++] = make_uint2(cw[1], __float_as_uint(k[1]));
-        if (k[0] < INFINITY) {
-          w = cw[0];
-          et = k[0];
-          have = true;
-        }
-      }
-    }
-  }
-  for (uint32_t i = 0; i < sc.n_planes; ++i) { /* geometry.zig:129-139 */
-    double th;
-    if (prim_t(sc.planes[i], o, d, tmin, closest, th)) {
-      closest = th;
-      best_k = -2 - (int32_t)i;
-    }
-  }
-  t_out = closest;
-  return best_k;
-}
-
-/* scene_occluded_fast over the 4-wide tree: every child reached is pushed
- * (the answer does not depend on the order), the walk stops at the first
- * primitive hit. */
-ZT_D bool scene_occluded_wide(const DevScene& sc, dv3 o, dv3 d, double tmin, double tmax) {
-  if (sc.has_root) {
-    FRay fr;
-    if (!fray_make(o, d, fr)) return scene_occluded_exact_outlined(sc, o, d, tmin, tmax);
-    const float tmin32 = __double2float_rd(tmin), tmax32 = __double2float_ru(tmax);
-    float t;
-    if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
-              tmin32, tmax32, t)) {
-      uint32_t stack[kWideStackSize];
-      uint32_t w = sc.wroot_word;
-      bool have = true;
-      int sp = 0;
-      for (;;) {
-        if (!have) {
-          if (sp == 0) break;
-          w = stack[--sp];
-        }
-        have = false;
-        const uint32_t cnt = w >> kFastCountShift, first = w & kFastFirstMask;
-        if (cnt > 0) {
-          for (uint32_t k = first; k < first + cnt; ++k) {
-            double th;
-            if (prim_t(sc.prims[k], o, d, tmin, tmax, th)) return true;
-          }
-          continue;
-        }
-        float k[4];
-        uint32_t cw[4];
-        wide_children(sc.wnodes + first, fr, tmin32, tmax32, k, cw);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (!(k[i] < INFINITY)) continue;
-          if (have) stack[sp++] = w;
-          w = cw[i];
-          have = true;
-        }
-      }
-    }
-  }
-  for (uint32_t i = 0; i < sc.n_planes; ++i) {
-    double th;
-    if (prim_t(sc.planes[i], o, d, tmin, tmax, th)) return true;
-  }
-  return false;
-}
-
 }  // namespace zt
 
 #endif

@@ -65,25 +65,6 @@ struct ZT_ALIGN(64) FPair {
   uint32_t word[2];
   uint32_t pad[2];
 };
-/* 128 bytes: one node of the 4-wide tree the fast walk traverses, collapsed
- * from the binary tree (each wide node holds up to four nodes of the binary
- * tree, its children being their children).  Boxes as in FPair (the binary
- * nodes' boxes, moved outward and rounded outward to float), stored axis by
- * axis so one 16-byte load brings one bound of all four children.  word[i]:
- * count << 28 | first for a leaf, the wide node's index for an interior
- * child, kWideEmpty for an unused slot. */
-struct ZT_ALIGN(128) WNode {
-  float lo[3][4];
-  float hi[3][4];
-  uint32_t word[4];
-  uint32_t pad[4];
-};
-constexpr uint32_t kWideEmpty = 0xFFFFFFFFu;
-/* Depth of the binary tree is at most 64 (bvh.zig: max_depth), so a wide
- * node is at most 64 levels deep and the walk holds at most 3 pending
- * children per level. */
-constexpr int kWideStackSize = 3 * 64 + 2;
-
 constexpr uint32_t kFastCountShift = 28;
 constexpr uint32_t kFastFirstMask = (1u << kFastCountShift) - 1;
 constexpr uint32_t kFastMaxLeaf = (1u << (32 - kFastCountShift)) - 1;
@@ -141,10 +122,8 @@ struct DevScene {
   DBackground bg;
   /* fast traversal (zt_fast.cuh): conservative float records and root box */
   const FPair* fpairs;
-  const WNode* wnodes;
   float froot_lo[3], froot_hi[3];
   uint32_t froot_word;
-  uint32_t wroot_word; /* the root as a wide-tree payload word */
   uint32_t fast_ok;   /* 1 when the fast records exist (leaves <= 15 primitives, bounds within kFastMaxCoord) */
 };
 

@@ -437,12 +437,7 @@ ZT_D double schlick(double cosine, double eta) { /* material.zig:66-70 */
 }
 
 /* Material.scatter, material.zig:34-62. */
-#if ZT_SCATTER_NOINLINE
-#define ZT_SCATTER_ATTR __device__ __noinline__
-#else
-#define ZT_SCATTER_ATTR ZT_D
-#endif
-ZT_SCATTER_ATTR bool material_scatter(const DMat& m, dv3 in_dir, const Hit& h, Rng& rng, dv3& atten, dv3& out_d) {
+ZT_D bool material_scatter(const DMat& m, dv3 in_dir, const Hit& h, Rng& rng, dv3& atten, dv3& out_d) {
   if (m.kind == kLambertian) {
     dv3 dir = h.normal + rng_unit_vector(rng);
     if (vnear_zero(dir)) dir = h.normal;
@@ -579,12 +574,7 @@ ZT_D double lights_pdf_hit(const DevScene& sc, dv3 origin, dv3 hit_point) {
 }
 
 /* ----------------------------------------------------------- Camera ---- */
-#if ZT_CAMERA_NOINLINE
-#define ZT_CAMERA_ATTR __device__ __noinline__
-#else
-#define ZT_CAMERA_ATTR ZT_D
-#endif
-ZT_CAMERA_ATTR void camera_ray(const DCamera& c, double s, double t, Rng& rng, dv3& ro, dv3& rd) { /* camera.zig:59-67 */
+ZT_D void camera_ray(const DCamera& c, double s, double t, Rng& rng, dv3& ro, dv3& rd) { /* camera.zig:59-67 */
   dv3 origin = L3(c.origin);
   if (c.lens_radius > 0) {
     const dv3 p = rng_in_unit_disk(rng);

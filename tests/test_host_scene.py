@@ -111,9 +111,17 @@ def test_device_entry_points_fail_loudly_without_a_gpu(native_lib):
     from zigtrace_b200 import scenes
     s = scenes.cornell().build()
     o = zt.Options(8, 8, 1, 4)
+    from zigtrace_b200 import sharding
+    fast = zt.GpuConfig(precision=zt.PRECISION_FAST)
     calls = [lambda: zt.render(s, o), lambda: zt.render_rgb8(s, o), lambda: zt.render_png(s, o),
-             lambda: zt.forward(s, o), lambda: zt.render_batch([s], [o])]
+             lambda: zt.forward(s, o), lambda: zt.render_batch([s], [o]), lambda: zt.render(s, o, fast),
+             lambda: zt.render_batch([s], [o], fast), lambda: sharding.render_rows(s, o, 0, 4),
+             lambda: zt.render(s, o, zt.GpuConfig(zt.MODE_WAVEFRONT_SORTED))]
     for call in calls:
         with pytest.raises(zt.ZigtraceError) as ei:
             call()
         assert ei.value.name == "CudaError"
+    # device-resident calls need an uploaded scene: rejected before any device work
+    with pytest.raises(zt.ZigtraceError) as ei:
+        zt.render_rows_device(s, o, 0, 4, 1 << 20, 0)
+    assert ei.value.name in ("CudaError", "InvalidArgument")

@@ -46,12 +46,17 @@ def fma32(a, b, c):
     return (a.astype(np.float64) * b.astype(np.float64) + c.astype(np.float64)).astype(F32)
 
 
-def f32_slab(lo32, hi32, o, d, tmin, tmax):
+def f32_slab(lo32, hi32, o, d, tmin, tmax, rcp_ulps=None):
+    """rcp_ulps: per-element -1/0/+1, the device reciprocal's error (it is
+    within 1 ulp of the correctly rounded one)."""
     o32, d32 = o.astype(F32), d.astype(F32)
     om = np.abs(o32).max(axis=1)
     K = np.where(om > F32(1e7), F32(1e37) / om, F32(1e30)).astype(F32)
     with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
         inv = F32(1) / d32
+        if rcp_ulps is not None:
+            inv = np.where(rcp_ulps > 0, np.nextafter(inv, F32(np.inf)),
+                           np.where(rcp_ulps < 0, np.nextafter(inv, F32(-np.inf)), inv)).astype(F32)
     inv = np.where(np.abs(inv) <= K[:, None], inv, np.copysign(K[:, None], inv)).astype(F32)
     n = (-o32 * inv).astype(F32)
     w = (np.abs(n) * F32(2.0 ** -20)).astype(F32)
@@ -111,7 +116,8 @@ def test_float_box_test_is_a_superset_of_the_f64_test():
             inv = 1.0 / d
         for tmin, tmax in ((1e-4, np.inf), (1e-4, 37.5), (0.0, 1e3)):
             hit64 = f64_slab(lo[k], hi[k], o, inv, tmin, tmax)
-            hit32, near32 = f32_slab(lo32[k], hi32[k], o, d, tmin, tmax)
+            hit32, near32 = f32_slab(lo32[k], hi32[k], o, d, tmin, tmax,
+                                     rcp_ulps=rng.integers(-1, 2, size=(len(o), 3)))
             missed = hit64 & ~hit32
             assert not missed.any(), f"{missed.sum()} boxes reached by the f64 test but not the float test"
             total_hits += int(hit64.sum())
@@ -129,7 +135,7 @@ def test_float_entry_distance_is_a_lower_bound():
         inv = 1.0 / d
     tmin = 1e-4
     hit64 = f64_slab(lo[k], hi[k], o, inv, tmin, np.inf)
-    _, near32 = f32_slab(lo32[k], hi32[k], o, d, tmin, np.inf)
+    _, near32 = f32_slab(lo32[k], hi32[k], o, d, tmin, np.inf, rcp_ulps=rng.integers(-1, 2, size=(len(o), 3)))
     near64 = np.full(len(o), tmin)
     with np.errstate(invalid="ignore", over="ignore"):
         for a in range(3):

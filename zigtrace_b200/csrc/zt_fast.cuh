@@ -13,16 +13,18 @@
  * reference's f64 test of the same box succeeds (same ray, same [tmin,
  * tmax]):
  *  - the ray is o + t d in f64; per axis the walk uses o32 = fl32(o),
- *    I = fl32(1 / fl32(d)) (clamped to +-K, below) and n = fl32(-o32 I), and
- *    computes a plane distance as fl32(c I + off) with one FMA, c the float
- *    plane and off = n -+ w.  Against the exact (c - o) / d the error is at
- *    most 2^-23 (1.5 |c| + 3 |o|) / |d| (rounding of d, of 1/d, of o, of the
- *    product n, of the FMA and of n -+ w, each at most 2^-24 relative);
+ *    I = rcp(fl32(d)) (the hardware reciprocal, within 1 ulp, i.e. 2^-23
+ *    relative; clamped to +-K, below) and n = fl32(-o32 I), and computes a
+ *    plane distance as fl32(c I + off) with one FMA, c the float plane and
+ *    off = n -+ w.  Against the exact (c - o) / d the error is at most
+ *    2^-23 (2 |c| + 3.5 |o|) / |d| (rounding of d, of o, of the product n,
+ *    of the FMA and of n -+ w, each at most 2^-24 relative, and the
+ *    reciprocal's 2^-23);
  *  - the |c| part is covered by the records: every bound is moved outward by
- *    eps = 2^-20 M (M the largest |bound| on that axis; 5x the 1.5 2^-23 M
+ *    eps = 2^-20 M (M the largest |bound| on that axis; 4x the 2 2^-23 M
  *    needed), which moves a near plane's distance down and a far plane's up
  *    by eps / |d|;
- *  - the |o| part is covered per ray: w = 2^-20 |n| (2.6x the 3 2^-23 |o I|
+ *  - the |o| part is covered per ray: w = 2^-20 |n| (2.3x the 3.5 2^-23 |o I|
  *    needed) is subtracted from near planes and added to far planes;
  *  - so each near distance is at most the exact one and each far distance at
  *    least the exact one, tmin is rounded down and tmax up, and an interval
@@ -69,7 +71,8 @@ ZT_D bool fray_make(dv3 o, dv3 d, FRay& r) {
   const float K = om > 1e7f ? 1e37f / om : 1e30f; /* K |o| <= 1e37, K * kFastMaxCoord <= 1e37 */
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    float inv = 1.0f / d3[a];
+    float inv;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(d3[a])); /* within 1 ulp; +-0 (and flushed subnormals) give +-inf */
     if (!(fabsf(inv) <= K)) inv = copysignf(K, inv); /* +-inf (a zero component) and huge values */
     const float n = -o3[a] * inv;
     const float w = fabsf(n) * 0x1.0p-20f;

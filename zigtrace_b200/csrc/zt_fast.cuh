@@ -41,7 +41,7 @@
  * superset of the leaves the reference tests; it differs from the
  * reference's only where two primitives tie, or where the reference's own
  * f64 box test misses a primitive hit by rounding (a grazing ray).  Images
- * are held to the north star's statistical bar (per-channel relative RMSE
+ * are held to a statistical bar (per-channel relative RMSE
  * and mean luminance against the oracle), not to bit equality.
  *
  * Stack entries are 8 bytes (packed payload word + float entry distance),

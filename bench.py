@@ -71,22 +71,26 @@ def roofline_entry(work: dict, samples: int, kernel_ms: float, sms: int, traffic
     achieved = flop / (kernel_ms / 1e3) / 1e12
     peak = sms * FP64_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
     peak32 = sms * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
-    busy = ((flop - f32) / (peak * 1e12) + f32 / (peak32 * 1e12)) / (kernel_ms / 1e3)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     bytes_per_launch = work["bytes"] * samples
     mixed = {}
+    peak_used = peak
     if f32 > 0:
+        # the rate this mix of f64 and f32 work would reach with each part at
+        # its own pipe's peak; achieved / that = the time-weighted fraction
+        peak_used = flop / ((flop - f32) / peak + f32 / peak32)
         mixed = {"bound": "fp64+fp32",
                  "split": {"fp64_tflops": round((flop - f32) / (kernel_ms / 1e3) / 1e12, 3),
                            "fp64_peak": round(peak, 1),
                            "fp32_tflops": round(f32 / (kernel_ms / 1e3) / 1e12, 3), "fp32_peak": round(peak32, 1),
                            "note": "box tests in f32 (FMA) against the nominal FP32 peak, primitives and shading "
-                                   "in f64 against the nominal FP64 peak; frac = time the arithmetic needs at "
-                                   "those peaks over the kernel's time"}}
+                                   "in f64 against the nominal FP64 peak; peak = the rate of this mix with each "
+                                   "part at its pipe's peak, so frac = the time the arithmetic needs at those "
+                                   "peaks over the kernel's time"}}
     return {
-        "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 1), "unit": "TFLOP/s",
-        "frac": round(busy, 4),
+        "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak_used, 1), "unit": "TFLOP/s",
+        "frac": round(achieved / peak_used, 4),
         **mixed,
         "traffic": traffic, "traffic_note": traffic_note, "ncu_execution": execution,
         "peak_source": f"nominal FP64: {sms} SMs x 64 lanes x 2 FLOP (FMA) x 1965 MHz; "

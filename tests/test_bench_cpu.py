@@ -85,6 +85,7 @@ def test_roofline_with_single_precision_box_tests():
     p32 = 148 * 128 * 2 * bench.NOMINAL_SM_MHZ * 1e6
     want = (120.0 * 1e7 / p64 + 480.0 * 1e7 / p32) / 5e-3
     assert r["bound"] == "fp64+fp32" and r["frac"] == pytest.approx(want, abs=1e-4)  # frac has 4 decimals
+    assert r["frac"] == pytest.approx(r["achieved"] / r["peak"], rel=1e-2)  # frac = achieved / peak
     assert r["split"]["fp32_tflops"] == pytest.approx(480.0 * 1e7 / 5e-3 / 1e12, rel=1e-3)
     assert "flop_f32" not in r["per_sample"]
 

@@ -379,7 +379,9 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
   dv3 sum = V(0, 0, 0);
   uint64_t sample = 0, depth = 0;
   bool done = !valid, fresh = valid;
-  dv3 ro = V(0, 0, 0), rd = V(0, 0, 0), radiance = V(0, 0, 0), throughput = V(1, 1, 1), prev_origin = V(0, 0, 0);
+  /* prev_origin (render.zig:66-70) is read only after a bounce, where it
+   * equals ro: ro stands in for it, as in trace_with */
+  dv3 ro = V(0, 0, 0), rd = V(0, 0, 0), radiance = V(0, 0, 0), throughput = V(1, 1, 1);
   double prev_pdf = 0;
   for (;;) {
     if (fresh) { /* render.zig:138-140: the next sample's camera ray */
@@ -392,7 +394,6 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
         camera_ray(p.cam, s, t, rng, ro, rd);
         radiance = V(0, 0, 0);
         throughput = V(1, 1, 1);
-        prev_origin = V(0, 0, 0);
         prev_pdf = 0;
         depth = 0;
       }
@@ -410,7 +411,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
         const DMat& mat = sc.mats[hit.material];
         const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
         if (vmaxc(le) > 0) {
-          const double wt = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, prev_origin, hit.point)) : 1.0;
+          const double wt = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, ro, hit.point)) : 1.0;
           radiance = radiance + vscale(vmul(throughput, le), wt);
         }
         if (mat.kind == kLambertian && use_nee)
@@ -421,7 +422,6 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
         } else {
           throughput = vmul(throughput, atten);
           prev_pdf = (use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
-          prev_origin = hit.point;
           ro = hit.point;
           rd = sd;
           if (depth + 1 >= kRouletteDepth) {

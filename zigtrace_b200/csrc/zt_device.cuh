@@ -625,8 +625,11 @@ template <bool kAux, bool kNee = true, bool kFast = false>
 ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_depth, bool use_nee_arg,
                     TraceAux* aux) {
   const bool use_nee = kNee && use_nee_arg;
+  /* The reference's prev_origin (render.zig:66-70) is read only when
+   * prev_pdf > 0, i.e. after a bounce, where it always equals the current
+   * ray's origin ro: ro stands in for it and keeps three doubles out of the
+   * registers that stay live across every traversal. */
   dv3 radiance = V(0, 0, 0), throughput = V(1, 1, 1);
-  dv3 prev_origin = V(0, 0, 0);
   double prev_pdf = 0;
   uint32_t n_ext = 0;
   if (kAux) aux->first_prim = -1;
@@ -642,7 +645,7 @@ ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_d
     /* Material.emitted, material.zig:26-32 */
     const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
     if (vmaxc(le) > 0) {
-      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, prev_origin, hit.point)) : 1.0;
+      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, ro, hit.point)) : 1.0;
       radiance = radiance + vscale(vmul(throughput, le), w);
     }
     if (mat.kind == kLambertian && use_nee)
@@ -651,7 +654,6 @@ ZT_D dv3 trace_with(const DevScene& sc, dv3 ro, dv3 rd, Rng& rng, uint64_t max_d
     if (!material_scatter(mat, rd, hit, rng, atten, sd)) break;
     throughput = vmul(throughput, atten);
     prev_pdf = (use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
-    prev_origin = hit.point;
     ro = hit.point;
     rd = sd;
     if (depth + 1 >= kRouletteDepth) {

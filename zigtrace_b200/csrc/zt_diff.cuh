@@ -68,7 +68,8 @@ ZT_D dv3 trace_diff(const DevScene& sc, const double* __restrict__ theta, dv3 ro
                     uint64_t max_depth, bool use_nee, bool kAdj, dv3 L_total, dv3 adj, double* grad,
                     bool warp_private) {
   dv3 radiance = V(0, 0, 0), tp = V(1, 1, 1), tp0 = V(1, 1, 1);
-  dv3 prev_origin = V(0, 0, 0);
+  /* prev_origin (render.zig:66-70) is read only after a bounce, where it
+   * equals ro: ro stands in for it, as in trace_with */
   double prev_pdf = 0;
   for (uint64_t depth = 0; depth < max_depth; ++depth) {
     Hit hit;
@@ -82,7 +83,7 @@ ZT_D dv3 trace_diff(const DevScene& sc, const double* __restrict__ theta, dv3 ro
     const bool emits = mat.kind == kEmissive && hit.front_face;
     const dv3 le0 = emits ? L3(mat.color) : V(0, 0, 0);
     if (vmaxc(le0) > 0) { /* emission with its MIS weight, render.zig:77-81 */
-      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, prev_origin, hit.point)) : 1.0;
+      const double w = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, ro, hit.point)) : 1.0;
       if (kAdj) grad_add(grad, warp_private, m, vmul(adj, vscale(tp, w)));
       radiance = radiance + vscale(vmul(tp, th), w);
     }
@@ -121,7 +122,6 @@ ZT_D dv3 trace_diff(const DevScene& sc, const double* __restrict__ theta, dv3 ro
     tp = vmul(tp, atten);
     tp0 = vmul(tp0, atten0);
     prev_pdf = (use_nee && mat.kind == kLambertian) ? fmax(vdot(sd, hit.normal), 0.0) / kPi : 0;
-    prev_origin = hit.point;
     ro = hit.point;
     rd = sd;
     if (depth + 1 >= kRouletteDepth) { /* roulette on the theta0 throughput */

@@ -480,15 +480,15 @@ static void make_fast_records(const zt_scene* s, FlatScene* f) {
     for (int c = 0; c < 2; ++c) {
       const HostNode& ch = s->nodes[nd.first + c];
       for (int k = 0; k < 3; ++k) {
-        pr.lo[c][k] = f32_down(ch.bmin[k] - eps[k]);
-        pr.hi[c][k] = f32_up(ch.bmax[k] + eps[k]);
+        pr.b[c][k][0] = f32_down(ch.bmin[k] - eps[k]);
+        pr.b[c][k][1] = f32_up(ch.bmax[k] + eps[k]);
       }
       pr.word[c] = word(nd.first + c);
     }
   }
   for (int k = 0; k < 3; ++k) {
-    v.froot_lo[k] = f32_down(s->nodes[0].bmin[k] - eps[k]);
-    v.froot_hi[k] = f32_up(s->nodes[0].bmax[k] + eps[k]);
+    v.froot[k][0] = f32_down(s->nodes[0].bmin[k] - eps[k]);
+    v.froot[k][1] = f32_up(s->nodes[0].bmax[k] + eps[k]);
   }
   v.froot_word = word(0);
   v.fast_ok = 1;

@@ -52,12 +52,37 @@
 
 namespace zt {
 
-/* Per-ray constants of the float slab test. */
+/* Per-ray constants of the float slab test, as packed f32x2 operands: per
+ * axis the reciprocal twice, and the offsets of the planes through a box's
+ * lower and upper bound (the FPair layout's order). */
 struct FRay {
-  float inv[3];
-  float off_lo[3]; /* offset of the plane through a box's lower bound on each axis */
-  float off_hi[3]; /* ... through its upper bound */
+  unsigned long long inv2[3];
+  unsigned long long off2[3];
 };
+
+ZT_D unsigned long long f2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+/* Both plane distances of one axis: fl32(c * inv + off) for c = lower and
+ * upper bound, each lane one FMA with a single rounding (as fmaf). */
+ZT_D void f2_planes(unsigned long long box, unsigned long long inv2, unsigned long long off2, float& a, float& b) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(box), "l"(inv2), "l"(off2));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+/* Three-input minimum and maximum (sm_100). */
+ZT_D float fmax3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+ZT_D float fmin3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
 
 /* Largest |origin| component the float test takes; rays from farther away
  * (a hit far out on an unbounded plane) use the f64 walk. */
@@ -76,10 +101,9 @@ ZT_D bool fray_make(dv3 o, dv3 d, FRay& r) {
     if (!(fabsf(inv) <= K)) inv = copysignf(K, inv); /* +-inf (a zero component) and huge values */
     const float n = -o3[a] * inv;
     const float w = fabsf(n) * 0x1.0p-20f;
-    r.inv[a] = inv;
     /* lower plane nearer when inv >= 0: it takes n - w, the upper plane n + w */
-    r.off_lo[a] = inv >= 0.0f ? n - w : n + w;
-    r.off_hi[a] = inv >= 0.0f ? n + w : n - w;
+    r.inv2[a] = f2_pack(inv, inv);
+    r.off2[a] = inv >= 0.0f ? f2_pack(n - w, n + w) : f2_pack(n + w, n - w);
   }
   return true;
 }
@@ -94,25 +118,27 @@ __device__ __noinline__ bool scene_occluded_exact_outlined(const DevScene& sc, d
   return scene_occluded(sc, o, d, tmin, tmax);
 }
 
-/* Float slab test of one box; tnear is the (lower-bound) entry distance. */
-ZT_D bool fslab(float lx, float ly, float lz, float hx, float hy, float hz, const FRay& r, float tmin, float tmax,
-                float& tnear) {
-  const float a0 = fmaf(lx, r.inv[0], r.off_lo[0]), b0 = fmaf(hx, r.inv[0], r.off_hi[0]);
-  const float a1 = fmaf(ly, r.inv[1], r.off_lo[1]), b1 = fmaf(hy, r.inv[1], r.off_hi[1]);
-  const float a2 = fmaf(lz, r.inv[2], r.off_lo[2]), b2 = fmaf(hz, r.inv[2], r.off_hi[2]);
-  const float n = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), tmin));
-  const float f = fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fminf(fmaxf(a2, b2), tmax));
+/* Float slab test of one box given as its three (lower, upper) axis pairs;
+ * tnear is the (lower-bound) entry distance. */
+ZT_D bool fslab(unsigned long long bx, unsigned long long by, unsigned long long bz, const FRay& r, float tmin,
+                float tmax, float& tnear) {
+  float a0, b0, a1, b1, a2, b2;
+  f2_planes(bx, r.inv2[0], r.off2[0], a0, b0);
+  f2_planes(by, r.inv2[1], r.off2[1], a1, b1);
+  f2_planes(bz, r.inv2[2], r.off2[2], a2, b2);
+  const float n = fmax3f(fminf(a0, b0), fminf(a1, b1), fmaxf(fminf(a2, b2), tmin));
+  const float f = fmin3f(fmaxf(a0, b0), fmaxf(a1, b1), fminf(fmaxf(a2, b2), tmax));
   tnear = n;
   return n <= f;
 }
 
-/* One 64-byte record: both children's boxes and payload words. */
+/* One 64-byte record: both children's axis pairs and payload words. */
 struct FRec {
-  float4 q0, q1, q2;
+  ulonglong2 q0, q1, q2;
   uint2 w;
 };
 ZT_D FRec frec_load(const FPair* p) {
-  const float4* q = reinterpret_cast<const float4*>(p);
+  const ulonglong2* q = reinterpret_cast<const ulonglong2*>(p);
   FRec r;
   r.q0 = __ldg(q);
   r.q1 = __ldg(q + 1);
@@ -120,12 +146,16 @@ ZT_D FRec frec_load(const FPair* p) {
   r.w = __ldg(reinterpret_cast<const uint2*>(q + 3));
   return r;
 }
-/* lo[0] = q0.x q0.y q0.z, lo[1] = q0.w q1.x q1.y, hi[0] = q1.z q1.w q2.x, hi[1] = q2.y q2.z q2.w */
+/* left x y = q0.x q0.y, left z = q1.x; right x = q1.y, right y z = q2.x q2.y */
 ZT_D bool fslab_left(const FRec& r, const FRay& fr, float tmin, float tmax, float& t) {
-  return fslab(r.q0.x, r.q0.y, r.q0.z, r.q1.z, r.q1.w, r.q2.x, fr, tmin, tmax, t);
+  return fslab(r.q0.x, r.q0.y, r.q1.x, fr, tmin, tmax, t);
 }
 ZT_D bool fslab_right(const FRec& r, const FRay& fr, float tmin, float tmax, float& t) {
-  return fslab(r.q0.w, r.q1.x, r.q1.y, r.q2.y, r.q2.z, r.q2.w, fr, tmin, tmax, t);
+  return fslab(r.q1.y, r.q2.x, r.q2.y, fr, tmin, tmax, t);
+}
+ZT_D bool fslab_root(const DevScene& sc, const FRay& fr, float tmin, float tmax, float& t) {
+  return fslab(f2_pack(sc.froot[0][0], sc.froot[0][1]), f2_pack(sc.froot[1][0], sc.froot[1][1]),
+               f2_pack(sc.froot[2][0], sc.froot[2][1]), fr, tmin, tmax, t);
 }
 
 /* Scene.intersect (scene.zig:108-116) with the BVH walked over the float
@@ -142,8 +172,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
     const float tmin32 = __double2float_rd(tmin);
     float cl32 = __double2float_ru(closest);
     float t;
-    if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
-              tmin32, cl32, t)) {
+    if (fslab_root(sc, fr, tmin32, cl32, t)) {
       uint2 stack[kStackSize]; /* (payload word, entry distance bits) */
       uint32_t w = sc.froot_word;
       float et = t;
@@ -210,8 +239,7 @@ ZT_D bool scene_occluded_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
     if (!fray_make(o, d, fr)) return scene_occluded_exact_outlined(sc, o, d, tmin, tmax);
     const float tmin32 = __double2float_rd(tmin), tmax32 = __double2float_ru(tmax);
     float t;
-    if (fslab(sc.froot_lo[0], sc.froot_lo[1], sc.froot_lo[2], sc.froot_hi[0], sc.froot_hi[1], sc.froot_hi[2], fr,
-              tmin32, tmax32, t)) {
+    if (fslab_root(sc, fr, tmin32, tmax32, t)) {
       uint32_t stack[kStackSize];
       uint32_t w = sc.froot_word;
       bool have = true;

@@ -56,12 +56,13 @@ struct ZT_ALIGN(128) DPair {
  * (zt_fast.cuh).  Boxes are single precision and conservative: every bound
  * is moved outward by eps[axis] = 2^-20 * max(|root lo|, |root hi|) on that
  * axis and then rounded outward to float, so the box contains the f64 box
- * with a margin that covers the float slab test's rounding.  word[c] packs
- * the child's payload: count << 28 | first (count 0: first is the record of
- * the child's own children). */
+ * with a margin that covers the float slab test's rounding.  Each axis of a
+ * child is a (lower, upper) pair in adjacent words, the operand layout of one
+ * packed f32x2 FMA that gives both plane distances.  word[c] packs the
+ * child's payload: count << 28 | first (count 0: first is the record of the
+ * child's own children). */
 struct ZT_ALIGN(64) FPair {
-  float lo[2][3];
-  float hi[2][3];
+  float b[2][3][2]; /* [child][axis][lower, upper] */
   uint32_t word[2];
   uint32_t pad[2];
 };
@@ -122,7 +123,7 @@ struct DevScene {
   DBackground bg;
   /* fast traversal (zt_fast.cuh): conservative float records and root box */
   const FPair* fpairs;
-  float froot_lo[3], froot_hi[3];
+  float froot[3][2]; /* root box, [axis][lower, upper] as in FPair */
   uint32_t froot_word;
   uint32_t fast_ok;   /* 1 when the fast records exist (leaves <= 15 primitives, bounds within kFastMaxCoord) */
 };

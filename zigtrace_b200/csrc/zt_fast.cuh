@@ -191,7 +191,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
         if (cnt > 0) {
           for (uint32_t k = first; k < first + cnt; ++k) {
             double th;
-            if (prim_t(sc.prims[k], o, d, tmin, closest, th)) {
+            if (bounded_t(sc.prims[k], o, d, tmin, closest, th)) {
               closest = th;
               best_k = (int32_t)k;
               cl32 = __double2float_ru(th);
@@ -220,7 +220,7 @@ ZT_D int32_t scene_query_fast(const DevScene& sc, dv3 o, dv3 d, double tmin, dou
   }
   for (uint32_t i = 0; i < sc.n_planes; ++i) { /* geometry.zig:129-139 */
     double th;
-    if (prim_t(sc.planes[i], o, d, tmin, closest, th)) {
+    if (plane_prim_t(sc.planes[i], o, d, tmin, closest, th)) {
       closest = th;
       best_k = -2 - (int32_t)i;
     }

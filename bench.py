@@ -38,21 +38,22 @@ NOMINAL_SM_MHZ = 1965.0
 # grows with the samples traced.  Keyed by (workload, precision); workloads
 # without a capture report null.
 NCU_DRAM_BYTES_PER_SAMPLE = {("triangle_heavy", "exact"): 2.527835e9 / (1920 * 1080 * 8),
-                             ("triangle_heavy", "fast"): (1.138160e9 + 1.444120e9) / (1920 * 1080 * 8)}
+                             ("triangle_heavy", "fast"): (1.308102e9 + 1.654117e9) / (1920 * 1080 * 8)}
 # What bounds the kernel instead of a pipe peak, from the same capture:
 # issue slots used, lanes active per warp instruction, FP64 pipe activity.
 NCU_EXECUTION = {("triangle_heavy", "exact"): {"issue_active_pct": 62.7, "lanes_per_warp_instruction": 8.27,
                                                "fp64_pipe_active_pct": 45.9, "l1_hit_pct": 72.2, "l2_hit_pct": 84.3},
-                 ("triangle_heavy", "fast"): {"issue_active_pct": 62.5, "lanes_per_warp_instruction": 7.38,
-                                              "fp64_pipe_active_pct": 31.6, "fma_pipe_active_pct": 9.2,
-                                              "l1_hit_pct": 76.2, "l2_hit_pct": 83.7},
+                 ("triangle_heavy", "fast"): {"issue_active_pct": 59.5, "lanes_per_warp_instruction": 7.19,
+                                              "fp64_pipe_active_pct": 31.5, "fma_pipe_active_pct": 8.7,
+                                              "l1_hit_pct": 75.9, "l2_hit_pct": 83.1,
+                                              "top_stall": "long_scoreboard 5.4 cycles per issue"},
                  ("batch", "exact"): {"issue_active_pct": 70.2, "lanes_per_warp_instruction": 14.23,
                                       "fp64_pipe_active_pct": 44.5, "l1_hit_pct": 82.9, "l2_hit_pct": 88.5},
-                 ("batch", "fast"): {"issue_active_pct": 59.5, "lanes_per_warp_instruction": 14.33,
-                                     "fp64_pipe_active_pct": 19.9, "l1_hit_pct": 80.4, "l2_hit_pct": 88.4,
-                                     "top_stall": "no_instruction 3.5 cycles per issue"}}
+                 ("batch", "fast"): {"issue_active_pct": 72.9, "lanes_per_warp_instruction": 14.32,
+                                     "fp64_pipe_active_pct": 25.6, "fma_pipe_active_pct": 16.0, "l1_hit_pct": 78.7,
+                                     "l2_hit_pct": 88.9, "top_stall": "long_scoreboard 2.9 cycles per issue"}}
 # The batched launch, captured whole (rank 0's batch, one launch), by precision.
-NCU_DRAM_BYTES_BATCH = {"exact": 0.160607e9 + 1.138117e9, "fast": 0.100172e9 + 1.266429e9}
+NCU_DRAM_BYTES_BATCH = {"exact": 0.160607e9 + 1.138117e9, "fast": 0.167182e9 + 2.485141e9}
 
 
 FP32_LANES_PER_SM = 128

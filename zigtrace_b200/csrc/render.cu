@@ -411,7 +411,7 @@ __device__ __forceinline__ void render_pixel_regen(const DevScene& sc, const Ren
         const DMat& mat = sc.mats[hit.material];
         const dv3 le = (mat.kind == kEmissive && hit.front_face) ? L3(mat.color) : V(0, 0, 0);
         if (vmaxc(le) > 0) {
-          const double wt = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit(sc, ro, hit.point)) : 1.0;
+          const double wt = prev_pdf > 0 ? power_weight(prev_pdf, lights_pdf_hit<kFast>(sc, ro, hit.point)) : 1.0;
           radiance = radiance + vscale(vmul(throughput, le), wt);
         }
         if (mat.kind == kLambertian && use_nee)
@@ -1556,11 +1556,20 @@ static std::vector<double> theta_host(const zt_scene* s, const double* colors) {
   return th;
 }
 
+/* The parameters on the device, from the stream-ordered pool (legacy
+ * default stream, as every per-call buffer of the differentiable pair). */
 static zt_status upload_theta(const std::vector<double>& th, double** d_theta) {
   const size_t n = th.empty() ? 3 : th.size();
-  ZT_CUDA(cudaMalloc((void**)d_theta, n * sizeof(double)), "allocate parameters");
-  if (!th.empty())
-    ZT_CUDA(cudaMemcpy(*d_theta, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice), "upload parameters");
+  zt_status rc = pool_alloc((void**)d_theta, n * sizeof(double), 0, "allocate parameters");
+  if (rc != ZT_OK) return rc;
+  if (!th.empty()) {
+    const cudaError_t e = cudaMemcpy(*d_theta, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      pool_free(*d_theta, 0);
+      *d_theta = nullptr;
+      return cuda_fail(e, "upload parameters");
+    }
+  }
   return ZT_OK;
 }
 
@@ -1614,16 +1623,19 @@ zt_status zt_forward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin, 
       else cudaGetLastError();
     }
   }
-  cudaError_t e = cudaMalloc((void**)&d_out, bytes);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
+  if ((rc = pool_alloc((void**)&d_out, bytes, 0, "allocate framebuffer")) != ZT_OK) {
+    pool_free(d_theta, 0);
+    return rc;
+  }
+  cudaError_t e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
   if (e == cudaSuccess) {
     k_forward_diff<128><<<persistent_grid(k_forward_diff<128>, 128, p.width * p.rows), 128>>>(
         launch_view(s), p, d_theta, d_out, cache.L, s->device->counter);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost);
-  cudaFree(d_theta);
-  cudaFree(d_out);
+  pool_free(d_theta, 0);
+  pool_free(d_out, 0);
   if (e != cudaSuccess) return cuda_fail(e, "zt_forward");
   if (cache.L) {
     cache.valid = true;
@@ -1681,9 +1693,14 @@ zt_status zt_backward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin,
   const size_t img_bytes = (size_t)(p.rows * o->width * 3) * sizeof(double);
   double *d_theta = nullptr, *d_img = nullptr, *d_grad = nullptr;
   if ((rc = upload_theta(th, &d_theta)) != ZT_OK) return rc;
-  cudaError_t e = cudaMalloc((void**)&d_img, img_bytes);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&d_grad, n_params * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpy(d_img, d_image, img_bytes, cudaMemcpyHostToDevice);
+  rc = pool_alloc((void**)&d_img, img_bytes, 0, "allocate image adjoint");
+  if (rc == ZT_OK) rc = pool_alloc((void**)&d_grad, n_params * sizeof(double), 0, "allocate gradients");
+  if (rc != ZT_OK) {
+    pool_free(d_theta, 0);
+    pool_free(d_img, 0);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(d_img, d_image, img_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(d_grad, 0, n_params * sizeof(double));
   if (e == cudaSuccess) e = cudaMemsetAsync(s->device->counter, 0, sizeof(unsigned int), 0);
   if (e == cudaSuccess) {
@@ -1699,9 +1716,9 @@ zt_status zt_backward_rows(zt_scene* s, const zt_options* o, uint64_t row_begin,
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(d_colors, d_grad, n_params * sizeof(double), cudaMemcpyDeviceToHost);
-  cudaFree(d_theta);
-  cudaFree(d_img);
-  cudaFree(d_grad);
+  pool_free(d_theta, 0);
+  pool_free(d_img, 0);
+  pool_free(d_grad, 0);
   if (e != cudaSuccess) return cuda_fail(e, "zt_backward");
   return ZT_OK;
 }

@@ -216,7 +216,7 @@ def reference_arm(args):
     samples = n_pix * o.spp
     value = samples / statistics.mean(times) / 1e6
     sample_desc = f"{n_pix} random pixels x {o.spp} spp ({samples} samples) per step"
-    print(json.dumps({
+    emit({
         "impl": "reference", "metric": "Msamples/s", "value": round(value, 4), "unit": "Msamples/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * statistics.mean(times), 3), "higher_is_better": True, "scaling": "weak",
@@ -226,7 +226,7 @@ def reference_arm(args):
                          "sample": sample_desc + "; C restatement of the reference CPU renderer (oracle/), "
                                                  "-O3 -ffp-contract=off, atomic tile scheduler"},
         "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }), flush=True)
+    })
 
 
 # -------------------------------------------------------------- clocks ----
@@ -330,14 +330,14 @@ def b200_arm(args):
     if args.shard == "rows":
         line = shard_rows_arm(args, world, rank, local_rank, barrier, allmax)
         if rank == 0:
-            print(json.dumps(line), flush=True)
+            emit(line)
         dist.destroy_process_group()
         return
     if args.workload in ("batch", "diff"):
         arm = batch_arm if args.workload == "batch" else diff_arm
         line = arm(args, world, rank, local_rank, barrier, allmax)
         if rank == 0:
-            print(json.dumps(line), flush=True)
+            emit(line)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -503,7 +503,7 @@ def b200_arm(args):
         torch.cuda.empty_cache()
         line["batch"] = batch_arm(sub, world, rank, local_rank, barrier, allmax)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     if world > 1:
         dist.destroy_process_group()
 
@@ -841,12 +841,38 @@ def diff_arm(args, world, rank, local_rank, barrier, allmax):
     return line
 
 
+def emit(line: dict) -> None:
+    """Prints the run's JSON line on the process's original standard output."""
+    out = _JSON_OUT if _JSON_OUT is not None else sys.stdout
+    print(json.dumps(line), file=out, flush=True)
+
+
+_JSON_OUT = None
+
+
 def main():
-    args = parse_args()
-    if args.impl == "reference":
-        reference_arm(args)
-    else:
-        b200_arm(args)
+    global _JSON_OUT
+    # Native libraries (NCCL prints a version banner from rank 0 when its
+    # first communicator comes up) write to file descriptor 1 directly; the
+    # contract is one JSON line on standard output, so descriptor 1 is pointed
+    # at standard error for the run and the line goes to a copy of the
+    # original.
+    sys.stdout.flush()
+    saved = os.dup(1)
+    _JSON_OUT = os.fdopen(os.dup(saved), "w")
+    os.dup2(2, 1)
+    try:
+        args = parse_args()
+        if args.impl == "reference":
+            reference_arm(args)
+        else:
+            b200_arm(args)
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)  # descriptor 1 as the caller had it
+        os.close(saved)
+        _JSON_OUT.close()
+        _JSON_OUT = None
 
 
 if __name__ == "__main__":

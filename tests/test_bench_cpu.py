@@ -115,3 +115,16 @@ def test_wavefront_queue_bytes():
                                          workmodel.WF_BYTES_SHADOW * 33) / 100 + workmodel.BYTES_PIXEL / 4)
     assert b == pytest.approx(want)
     assert 700 < b < 1000  # the 1M-triangle workload's counters give about 830 bytes per sample
+
+
+def test_native_stdout_writes_do_not_mix_with_the_json_line():
+    """Libraries that write to descriptor 1 themselves (NCCL's version banner
+    on rank 0) land on standard error; standard output carries the JSON line
+    alone, and descriptor 1 is restored when main() returns."""
+    code = ("import os, sys; sys.path.insert(0, '.'); import bench; "
+            "bench.reference_arm = lambda args: (os.write(1, b'NCCL version banner\\n'), bench.emit({'metric': 'm'})); "
+            "sys.argv = ['bench.py', '--impl', 'reference']; bench.main(); print('AFTER_MAIN')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.splitlines() == ['{"metric": "m"}', "AFTER_MAIN"]
+    assert "NCCL version banner" in r.stderr

@@ -323,11 +323,13 @@ __device__ __forceinline__ void render_pixel(const DevScene& sc, const RenderPar
 /* Persistent megakernel: each warp takes an 8x4 pixel tile from the device
  * work counter until the image is exhausted (the device form of
  * Context.work's atomic tile counter, render.zig:113-119), so its camera rays
- * are coherent.  896 resident threads per SM (7 blocks of 128, <= 73
- * registers) measured fastest on the 1M-triangle workload among 512..1024.
+ * are coherent.  The exact instance with light sampling is built for 1024
+ * resident threads per SM (64 registers): on the 1M-triangle terrain 731
+ * Msamples/s against 722 at 896 (an earlier source measured 896 fastest).
  * The instance without light sampling (kNee = false) is a separate build
- * with its own residency. */
-constexpr int kMegaThreadsPerSm = 896;
+ * with its own residency: 896 threads (72 registers), equal to 1024 on the
+ * random spheres (2798 against 2794). */
+constexpr int kMegaThreadsPerSm = 1024;
 constexpr int kMegaThreadsPerSmNoNee = 896;
 #ifndef ZT_FAST_THREADS_PER_SM
 #define ZT_FAST_THREADS_PER_SM 1024
